@@ -1,0 +1,301 @@
+#!/usr/bin/env python3
+"""Throughput of the WCSPH step in particle-steps/s on B200.
+
+Workload (default): the 1,048,576-particle tilting-box scene (preset
+"large_tilting": r = 0.004, jitter +-0.2 r, N(0, 0.1) velocities, 2 x 1 x 1 m
+box tilting 0 -> 15 deg about z over 1 s, fixed dt 5e-4). A step is one
+FluidSimulator::update (sort, neighbourhood search, density, pressure,
+non-pressure force, integrate + collision, CFL reduction) plus the box update
+of that step.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 runs under torchrun as independent replicas (one scene per GPU, no
+data-path collective; scaling "weak"); time is the max over ranks.
+`--impl reference` times the reference's own CUDA kernels (compiled from its
+sources into oracle/_ref by oracle/build_ref.py) on the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT / "fluid-simulation_b200"))
+
+METRIC = "particle-steps/s"
+# Algorithmic bytes per particle of each pass (compulsory reads + writes of
+# the pass's own inputs/outputs, neighbour reads assumed cache-served).
+PASS_BYTES = {
+    "density_pass": 16 + 8,                       # pos -> rho, p
+    "force_pass": 16 + 16 + 4 + 4 + 16 * 3,       # pos, vel, rho, p -> a_p, n, vlap
+    "surface_integrate_pass": 16 * 6 + 4 + 16 * 3,  # pos, vel, n, rho, a_p, vlap -> a_np, pos, vel
+    "keys_hist": 16 + 8,
+    "radix_sort": 24,
+    "reorder_cells": 4 + 32 + 32 + 8 + 4,
+}
+STEP_BYTES = 400  # algorithmic bytes per fluid particle-step of the reference step structure
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d.get("hbm_gbs", 6650.0)), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if len(r) > 8 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 8 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            if len(r) > 8:
+                for k, name in enumerate(names):
+                    if r[5 + k].lower().startswith("active"):
+                        reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=None)
+    return world, rank, local, dist
+
+
+def max_over_ranks(value: float, dist, device) -> float:
+    if dist is None:
+        return value
+    import torch
+
+    t = torch.tensor([value], dtype=torch.float64, device=f"cuda:{device}")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(dist, device):
+    if dist is not None:
+        import torch
+
+        dist.barrier(device_ids=[device])
+
+
+def cpu_baseline(pre, budget_s: float = 15.0):
+    """FP64 oracle (own C restatement) on the host cores, bounded sample."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle
+
+    p, bx = pre.params, pre.box
+    pos, vel = pre.pos.copy(), pre.vel.copy()
+    bs, bm = (oracle.boundary_init(p, pre.bpos) if pre.bpos is not None else (None, None))
+    steps = 0
+    t0 = time.perf_counter()
+    while True:
+        r = oracle.step(p, bx, pos, vel, bs, bm, delta=pre.info.delta, nbr_cap=pos.shape[0] * 64)
+        pos = r.pos.astype(np.float32)
+        vel = r.vel.astype(np.float32)
+        steps += 1
+        el = time.perf_counter() - t0
+        if el > budget_s or steps >= 50:
+            break
+    return {"value": pre.info.fluid_n * steps / el, "unit": METRIC, "cores": oracle.num_threads(), "kind": "port",
+            "sample": f"{steps} FP64 oracle steps of the same {pre.info.fluid_n}-particle workload, "
+                      f"{el:.1f} s wall"}
+
+
+def run_ours(args, world, rank, local, dist):
+    import torch
+
+    import wcsph
+
+    torch.cuda.set_device(local)
+    pre = wcsph.preset(args.workload, seed=args.seed)
+    n = pre.info.fluid_n
+    delta = pre.info.delta
+    sim = pre.simulator(device=local)
+    stream = torch.cuda.ExternalStream(sim.stream_handle(), device=f"cuda:{local}")
+    boxes = [pre.box_at(k + 1) for k in range(args.warmup + args.steps + 8)] if pre.info.moving_box else None
+
+    def one(k):
+        if boxes is not None:
+            sim.set_box(boxes[k])
+        sim.step_n(1, delta)
+
+    for k in range(args.warmup):
+        one(k)
+    sim.synchronize()
+    barrier(dist, local)
+    torch.cuda.synchronize(local)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        for k in range(args.warmup, args.warmup + args.steps):
+            one(k)
+        e1.record(stream)
+        e1.synchronize()
+    sim.synchronize()
+    torch.cuda.synchronize(local)
+    ms = e0.elapsed_time(e1)
+    ms_max = max_over_ranks(ms, dist, local)
+    barrier(dist, local)
+
+    # per-pass device times (events between stages) for the roofline
+    stages = {}
+    for _ in range(5):
+        for k, v in sim.kernel_timings().items():
+            stages.setdefault(k, []).append(v)
+    stage_ms = {k: statistics.median(v) for k, v in stages.items()}
+
+    # end-to-end through the C ABI with host buffers: upload the state from
+    # pinned host memory, per step upload the box and read back the metrics,
+    # download the state at the end
+    pin_pos = torch.from_numpy(pre.pos).pin_memory()
+    pin_vel = torch.from_numpy(pre.vel).pin_memory()
+    out_pos = torch.empty_like(pin_pos).pin_memory()
+    out_vel = torch.empty_like(pin_vel).pin_memory()
+    sim.synchronize()
+    t0 = time.perf_counter()
+    sim.set_state(pin_pos.numpy(), pin_vel.numpy())
+    for k in range(args.steps):
+        if boxes is not None:
+            sim.set_box(boxes[k])
+        sim.update(delta)
+        sim.compute_state_metrics()
+    p_, v_ = sim.get_state()
+    out_pos.numpy()[:] = p_
+    out_vel.numpy()[:] = v_
+    e2e_s = time.perf_counter() - t0
+    e2e_s = max_over_ranks(e2e_s, dist, local)
+    box_bytes = 160
+    h2d = (32 * n + args.steps * (box_bytes if boxes is not None else 0)) / args.steps
+    d2h = (32 * n + 8 * args.steps) / args.steps
+
+    launches = sim.launches_per_step() * args.steps
+    sim.close()
+    if rank != 0:
+        return None
+    peak, peak_kind = measured_peaks()
+    dom = max(("density_pass", "force_pass", "surface_integrate_pass"), key=lambda k: stage_ms.get(k, 0.0))
+    dom_ms = stage_ms[dom]
+    achieved = PASS_BYTES[dom] * n / (dom_ms * 1e-3) / 1e9
+    value = world * n * args.steps / (ms_max * 1e-3)
+    step_bw = STEP_BYTES * n / (ms_max / args.steps * 1e-3) / 1e9
+    clocks = clk.summary()
+    line = {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic: seeded jittered lattice + N(0,0.1) velocities (preset large_tilting)",
+        "config": {"workload": args.workload, "particles": n, "dt": delta, "box": "2x1x1 m tilting 0->15 deg/1 s",
+                   "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (~250 MB resident per step)",
+                   "step_algorithmic_bytes_per_particle": STEP_BYTES,
+                   "step_hbm_fraction_of_" + peak_kind: step_bw / peak},
+        "clocks": {"sm_mhz": clocks["sm_mhz"], "sm_max_mhz": clocks["sm_max_mhz"], "reasons": clocks["reasons"]},
+        "e2e": {"value": world * n * args.steps / e2e_s, "unit": METRIC, "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h},
+        "gpu_launches": launches,
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_source": peak_kind, "traffic": None,
+                     "stage_ms": stage_ms},
+    }
+    if not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(pre, args.cpu_budget)
+    return line
+
+
+def run_reference(args, world, rank, local, dist):
+    if rank != 0:
+        return None
+    sys.path.insert(0, str(ROOT / "oracle"))
+    try:
+        import refpath
+    except Exception as e:  # noqa: BLE001
+        return {"impl": "reference", "unavailable": f"reference harness not importable: {e}"}
+    return refpath.bench_line(args, METRIC)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="large_tilting")
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-budget", type=float, default=15.0)
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    world, rank, local, dist = dist_setup()
+    try:
+        if args.impl == "reference":
+            line = run_reference(args, world, rank, local, dist)
+        else:
+            line = run_ours(args, world, rank, local, dist)
+        if rank == 0 and line is not None:
+            print(json.dumps(line), flush=True)
+    finally:
+        if dist is not None:
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,251 @@
+// radix_sort.cu — see radix_sort.cuh for the design.
+#include "radix_sort.cuh"
+
+#include <cuda/atomic>
+
+namespace wcsph {
+
+namespace {
+__device__ __forceinline__ u32 lanemask_lt() {
+    u32 m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+// Warp-aggregated shared-memory increment of 8 digit histograms for one key
+// per lane. Many lanes share digits (keys arrive nearly sorted), so each
+// distinct digit value gets one atomic.
+__device__ __forceinline__ void hist_add_key(u32 (*s_hist)[256], u64 key, bool valid) {
+    const u32 lane = threadIdx.x & 31;
+#pragma unroll
+    for (int p = 0; p < SORT_DIGITS; ++p) {
+        const u32 d = valid ? static_cast<u32>((key >> (8 * p)) & 255u) : 256u;
+        const u32 peers = __match_any_sync(0xffffffffu, d);
+        const u32 leader = __ffs(peers) - 1;
+        if (valid && lane == leader) atomicAdd(&s_hist[p][d], static_cast<u32>(__popc(peers)));
+    }
+}
+
+__device__ __forceinline__ void flush_hist(u32 (*s_hist)[256], u32* hist) {
+    for (int t = threadIdx.x; t < SORT_DIGITS * 256; t += blockDim.x) {
+        const u32 c = (&s_hist[0][0])[t];
+        if (c) atomicAdd(hist + t, c);
+    }
+}
+}  // namespace
+
+__global__ void keys_hist_kernel(const float4* __restrict__ pos, u32 n, float cs,
+                                 u64* __restrict__ keys_out, u32* __restrict__ hist) {
+    __shared__ u32 s_hist[SORT_DIGITS][256];
+    for (int t = threadIdx.x; t < SORT_DIGITS * 256; t += blockDim.x) (&s_hist[0][0])[t] = 0;
+    __syncthreads();
+    const u32 stride = gridDim.x * blockDim.x;
+    // The loop trip count is uniform across the warp (match.any needs all lanes).
+    for (u32 base = blockIdx.x * blockDim.x; base < n; base += stride) {
+        const u32 i = base + threadIdx.x;
+        const bool valid = i < n;
+        u64 key = 0;
+        if (valid) {
+            key = morton_key(cell_of(pos[i], cs));
+            keys_out[i] = key;
+        }
+        hist_add_key(s_hist, key, valid);
+    }
+    __syncthreads();
+    flush_hist(s_hist, hist);
+}
+
+__global__ void hist_only_kernel(const u64* __restrict__ keys, u32 n, u32* __restrict__ hist) {
+    __shared__ u32 s_hist[SORT_DIGITS][256];
+    for (int t = threadIdx.x; t < SORT_DIGITS * 256; t += blockDim.x) (&s_hist[0][0])[t] = 0;
+    __syncthreads();
+    const u32 stride = gridDim.x * blockDim.x;
+    for (u32 base = blockIdx.x * blockDim.x; base < n; base += stride) {
+        const u32 i = base + threadIdx.x;
+        const bool valid = i < n;
+        const u64 key = valid ? keys[i] : 0ull;
+        hist_add_key(s_hist, key, valid);
+    }
+    __syncthreads();
+    flush_hist(s_hist, hist);
+}
+
+// One CTA of 256 threads: thread t owns digit value t of every pass.
+__global__ void sort_plan_kernel(u32 n, u32* __restrict__ hist, u32* __restrict__ offsets,
+                                 DevState* __restrict__ st) {
+    __shared__ u32 s_scan[256];
+    __shared__ u32 s_max[8];
+    __shared__ u32 s_active[SORT_DIGITS];
+    const u32 t = threadIdx.x;
+    for (int p = 0; p < SORT_DIGITS; ++p) {
+        const u32 c = hist[p * 256 + t];
+        hist[p * 256 + t] = 0;  // ready for the next sort
+        // block exclusive scan (Hillis-Steele over 256 entries)
+        s_scan[t] = c;
+        __syncthreads();
+        for (u32 o = 1; o < 256; o <<= 1) {
+            const u32 v = t >= o ? s_scan[t - o] : 0u;
+            __syncthreads();
+            s_scan[t] += v;
+            __syncthreads();
+        }
+        offsets[p * 256 + t] = s_scan[t] - c;
+        // max bucket: a pass is trivial when one bucket holds every key
+        u32 m = c;
+        for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+        if ((t & 31) == 0) s_max[t >> 5] = m;
+        __syncthreads();
+        if (t == 0) {
+            u32 mx = 0;
+            for (int w = 0; w < 8; ++w) mx = max(mx, s_max[w]);
+            s_active[p] = (n > 0 && mx < n) ? 1u : 0u;
+        }
+        __syncthreads();
+    }
+    if (t == 0) {
+        u32 sel = 0;
+        u32 first = SORT_DIGITS;
+        for (int p = 0; p < SORT_DIGITS; ++p) {
+            st->sort_active[p] = s_active[p];
+            st->sort_sel[p] = sel;
+            st->sort_tile_counter[p] = 0;
+            if (s_active[p]) {
+                if (first == SORT_DIGITS) first = p;
+                sel = (sel == 1u) ? 2u : 1u;
+            }
+        }
+        st->sort_sel[SORT_DIGITS] = sel;
+        st->first_active = first;
+    }
+}
+
+__global__ void __launch_bounds__(SORT_THREADS)
+onesweep_kernel(u32 n, int pass, u64* __restrict__ k0, u64* __restrict__ k1, u64* __restrict__ k2,
+                u32* __restrict__ v1, u32* __restrict__ v2, const u32* __restrict__ offsets,
+                u32* __restrict__ lookback, u32 tiles, DevState* __restrict__ st) {
+    if (!st->sort_active[pass]) return;
+    constexpr int NW = SORT_THREADS / 32;
+    __shared__ u32 s_tile;
+    __shared__ u32 s_wcnt[NW][256];
+    __shared__ u32 s_base[256];
+
+    const u32 sel_in = st->sort_sel[pass];
+    const u32 sel_out = (sel_in == 1u) ? 2u : 1u;
+    const u64* keys_in = sel_in == 0 ? k0 : (sel_in == 1 ? k1 : k2);
+    const u32* vals_in = sel_in == 0 ? nullptr : (sel_in == 1 ? v1 : v2);
+    u64* keys_out = sel_out == 1 ? k1 : k2;
+    u32* vals_out = sel_out == 1 ? v1 : v2;
+    const int shift = 8 * pass;
+
+    const u32 tid = threadIdx.x;
+    const u32 lane = tid & 31;
+    const u32 warp = tid >> 5;
+    if (tid == 0) s_tile = atomicAdd(&st->sort_tile_counter[pass], 1u);
+    for (int t = tid; t < NW * 256; t += SORT_THREADS) (&s_wcnt[0][0])[t] = 0;
+    __syncthreads();
+    const u32 tile = s_tile;
+    if (tile >= tiles) return;  // cannot happen: grid == tiles
+
+    u64 key[SORT_IPT];
+    u32 val[SORT_IPT];
+    u32 dig[SORT_IPT];
+    u32 rank[SORT_IPT];
+    const u32 wbase = tile * SORT_TILE + warp * (32 * SORT_IPT);
+#pragma unroll
+    for (int k = 0; k < SORT_IPT; ++k) {
+        const u32 idx = wbase + k * 32 + lane;
+        if (idx < n) {
+            key[k] = keys_in[idx];
+            val[k] = vals_in ? vals_in[idx] : idx;
+            dig[k] = static_cast<u32>((key[k] >> shift) & 255u);
+        } else {
+            key[k] = 0;
+            val[k] = 0;
+            dig[k] = 256u;
+        }
+    }
+    // Stable warp-level ranking: items are warp-striped so (k, lane) order is
+    // the input order within the warp's 256-key segment.
+    const u32 lt = lanemask_lt();
+#pragma unroll
+    for (int k = 0; k < SORT_IPT; ++k) {
+        const u32 d = dig[k];
+        const u32 peers = __match_any_sync(0xffffffffu, d);
+        const u32 before = __popc(peers & lt);
+        u32 base = 0;
+        if (d < 256u) base = s_wcnt[warp][d];
+        rank[k] = base + before;
+        __syncwarp();
+        if (d < 256u && (peers >> lane) == 1u)  // highest lane of the peer group
+            s_wcnt[warp][d] = base + __popc(peers);
+        __syncwarp();
+    }
+    __syncthreads();
+
+    // Thread t = digit t: exclusive prefix over warps, tile total, look-back.
+    {
+        const u32 d = tid;
+        u32 running = 0;
+#pragma unroll
+        for (int w = 0; w < NW; ++w) {
+            const u32 c = s_wcnt[w][d];
+            s_wcnt[w][d] = running;
+            running += c;
+        }
+        const u32 count = running;
+        u32* lb = lookback + (static_cast<size_t>(pass) * tiles) * 256u;
+        cuda::atomic_ref<u32, cuda::thread_scope_device> mine(lb[static_cast<size_t>(tile) * 256u + d]);
+        u32 excl = 0;
+        if (tile == 0) {
+            mine.store(LB_FLAG_INC | count, cuda::memory_order_relaxed);
+        } else {
+            mine.store(LB_FLAG_AGG | count, cuda::memory_order_relaxed);
+            int pred = static_cast<int>(tile) - 1;
+            u32 spins = 0;
+            while (pred >= 0) {
+                cuda::atomic_ref<u32, cuda::thread_scope_device> other(
+                    lb[static_cast<size_t>(pred) * 256u + d]);
+                const u32 v = other.load(cuda::memory_order_relaxed);
+                const u32 flag = v & ~LB_VALUE_MASK;
+                if (flag == 0u) {
+                    if (++spins > LB_SPIN_LIMIT) {  // bounded wait: flag the error, never hang
+                        atomicOr(&st->error_flags, ERR_LOOKBACK_TIMEOUT);
+                        break;
+                    }
+                    continue;
+                }
+                excl += v & LB_VALUE_MASK;
+                if (flag == LB_FLAG_INC) break;
+                --pred;
+            }
+            mine.store(LB_FLAG_INC | (excl + count), cuda::memory_order_relaxed);
+        }
+        s_base[d] = offsets[pass * 256 + d] + excl;
+    }
+    __syncthreads();
+
+#pragma unroll
+    for (int k = 0; k < SORT_IPT; ++k) {
+        const u32 d = dig[k];
+        if (d < 256u) {
+            const u32 dst = s_base[d] + s_wcnt[warp][d] + rank[k];
+            if (dst < n) {  // always true unless a look-back wait gave up
+                keys_out[dst] = key[k];
+                vals_out[dst] = val[k];
+            }
+        }
+    }
+}
+
+void enqueue_sort_passes(const SortBuffers& b, u32 n, DevState* st, cudaStream_t stream) {
+    const u32 tiles = sort_tiles(n);
+    if (n == 0) return;
+    sort_plan_kernel<<<1, 256, 0, stream>>>(n, b.hist, b.offsets, st);
+    cudaMemsetAsync(b.lookback, 0, sizeof(u32) * SORT_DIGITS * static_cast<size_t>(tiles) * 256u, stream);
+    for (int p = 0; p < SORT_DIGITS; ++p)
+        onesweep_kernel<<<tiles, SORT_THREADS, 0, stream>>>(n, p, b.keys[0], b.keys[1], b.keys[2],
+                                                            b.vals[1], b.vals[2], b.offsets, b.lookback,
+                                                            tiles, st);
+}
+
+}  // namespace wcsph

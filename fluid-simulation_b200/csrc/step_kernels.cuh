@@ -1,0 +1,96 @@
+// step_kernels.cuh — the neighbourhood search and SPH force kernels of one
+// WCSPH step (everything after the sort).
+//
+//   reorder_cells   gather pos/vel into sorted order + mark cell runs + insert
+//                   cells into the linear-probed hash (cell_start/cell_end)
+//                   (particle_data.cuh:130-131 + rebuild_n_search.cu:10-36)
+//   density pass    rho, Tait p (+boundary) and the per-particle neighbour
+//                   bitmasks over the home cell's candidate list
+//                   (compute_rho_p[_with_boundary], compute_rho_p.cu:192-318)
+//   force pass      pressure accel (+boundary), normals, viscosity Laplacian
+//                   (compute_pressure_accel_n_normal.cu:240-366 and the
+//                   viscosity half of compute_non_pressure_accel.cu:114-144)
+//   surface pass    surface tension, a_np, symplectic Euler + box collision,
+//                   CFL max |v|^2 and metric reductions
+//                   (compute_non_pressure_accel.cu + update_positions.cu:14-68)
+//
+// Work decomposition (all three passes): one warp per 32-particle chunk of
+// the sorted array; for every cell that starts inside the chunk, the warp
+// looks up the (2R+1)^3 neighbour cells once (lane-parallel hash probes),
+// expands their contiguous particle ranges into a shared-memory candidate
+// list, and assigns L = 32/next_pow2(n_home) lanes to each home particle.
+// Lanes stride the candidate list; partial sums are combined with xor
+// shuffles inside each L-lane group.
+#pragma once
+#include "sph_common.cuh"
+
+namespace wcsph {
+
+constexpr int TRAV_WARPS = 4;            // warps per block of the traversal passes
+constexpr int MAX_RANGE_CELLS = 125;     // (2R+1)^3 with R <= 2
+constexpr int MAX_BOUNDARY_CELLS = 125;
+
+struct HashView {
+    const u64* table;
+    const u32* cstart;
+    const u32* cend;
+    u32 tmask;
+};
+
+struct TravArgs {
+    u32 n;                    // fluid particles
+    const float4* pos;        // sorted positions
+    const float4* vel;        // sorted velocities
+    const u64* ckey;          // packed cell key per sorted particle
+    HashView fluid;
+    int range;                // R
+    // boundary
+    u32 nb;
+    const float4* bpos;
+    const float* bmass;
+    HashView boundary;
+    // neighbour bitmasks
+    u32* mask;
+    u32 mask_words;           // words per particle (candidate cap = 32*mask_words)
+    // fields
+    float* rho;
+    float* prs;
+    float4* ap;
+    float4* normal;
+    float4* vlap;
+    float4* anp;
+    // integrate outputs (state buffers)
+    float4* pos_out;
+    float4* vel_out;
+    DevBox* box;              // device copy of the collision box
+    DevState* st;
+    float delta;              // requested step (host value)
+    float cfl_factor;
+    float max_dt, min_dt, np_max_dt;
+    float metric_mass;        // host-side PARTICLE_MASS used by the ke metric
+    float* block_partials;    // [gridDim.x][2] sum|v|, sum|v|^2
+    u32* counts;              // neighbour export: counts
+    const u32* offsets;       // neighbour export: offsets
+    u32* nbr_out;             // neighbour export: indices
+    unsigned long long nbr_capacity;
+};
+
+enum PassKind : int { PASS_DENSITY = 0, PASS_FORCE = 1, PASS_SURFACE = 2, PASS_COUNT = 3, PASS_FILL = 4 };
+
+void launch_reorder_cells(const float4* pos_in, const float4* vel_in, const u32* perm_src1,
+                          const u32* perm_src2, const DevState* st, u32 n, float cs, float4* pos_out,
+                          float4* vel_out, u32* perm_out, u64* ckey_out, u64* table, u32* cstart,
+                          u32* cend, u32 tmask, DevState* st_err, cudaStream_t stream);
+
+void launch_pass(int kind, const DevParams& P, const TravArgs& a, cudaStream_t stream, int warps_per_block);
+u32 pass_grid(u32 n, int warps_per_block);
+
+// CFL max |v|^2 of a velocity array into st->vmax2_bits[st->parity].
+void launch_init_cfl(const float4* vel, u32 n, DevState* st, cudaStream_t stream);
+// Boundary masses (compute_boundary_mass.cu:10-30), per-thread, init only.
+void launch_boundary_mass(const DevParams& P, const float4* bpos, u32 nb, HashView bh, float* bmass,
+                          cudaStream_t stream);
+// Metrics of an arbitrary velocity array (used after load/reset).
+void launch_metrics(const float4* vel, u32 n, float mass, float* out2, cudaStream_t stream);
+
+}  // namespace wcsph

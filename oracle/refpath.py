@@ -1,0 +1,145 @@
+"""ctypes driver of the reference-kernel harness (oracle/_ref/<variant>).
+
+TEST AND BASELINE INFRASTRUCTURE: runs the reference's own CUDA kernels
+(compiled from its sources by oracle/build_ref.py) replaying its step.
+Used by the parity tests, tests/golden/make_ref_fixtures.py and
+`bench.py --impl reference`; never by the product.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import json
+import statistics
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+REF_DIR = HERE / "_ref"
+
+
+def available(variant: str) -> bool:
+    return (REF_DIR / variant / "librefpath.so").exists()
+
+
+def box_floats(box) -> np.ndarray:
+    """wcsph.Box -> 38 floats: min[3], max[3], model[16], model_inv[16]."""
+    return np.array(list(box.min) + list(box.max) + list(box.model) + list(box.model_inv), np.float32)
+
+
+class RefSim:
+    """One reference-path simulation (one per process: the harness is a singleton)."""
+
+    def __init__(self, variant: str, pos, vel, bpos, box, device: int = 0):
+        path = REF_DIR / variant / "librefpath.so"
+        if not path.exists():
+            raise OSError(f"reference harness {path} not built (oracle/build_ref.py)")
+        L = C.CDLL(str(path))
+        vp = C.c_void_p
+        L.ref_create.argtypes = [vp, vp, C.c_uint, vp, C.c_uint, vp, C.c_int]
+        L.ref_step.argtypes = [C.c_float]
+        L.ref_set_box.argtypes = [vp]
+        L.ref_time_steps.argtypes = [C.c_int, C.c_float, vp]
+        L.ref_time_steps.restype = C.c_float
+        L.ref_get_fields.argtypes = [vp] * 12 + [C.c_ulonglong, vp, vp]
+        L.ref_get_hash.argtypes = [vp, vp, vp, vp]
+        L.ref_get_boundary.argtypes = [vp, vp]
+        self.L = L
+        self.n = pos.shape[0]
+        self.nb = 0 if bpos is None else bpos.shape[0]
+        self._pos = np.ascontiguousarray(pos, np.float32)
+        self._vel = np.ascontiguousarray(vel, np.float32)
+        self._bpos = None if bpos is None else np.ascontiguousarray(bpos, np.float32)
+        b = box_floats(box)
+        st = L.ref_create(self._pos.ctypes.data, self._vel.ctypes.data, self.n,
+                          None if self._bpos is None else self._bpos.ctypes.data, self.nb, b.ctypes.data, device)
+        if st != 0:
+            raise RuntimeError(f"ref_create failed ({st}): variant {variant} was built for other particle counts")
+
+    def step(self, delta: float):
+        if self.L.ref_step(delta) != 0:
+            raise RuntimeError("ref_step failed")
+
+    def set_box(self, box):
+        b = box_floats(box)
+        self.L.ref_set_box(b.ctypes.data)
+
+    def time_steps(self, k: int, delta: float, boxes=None) -> float:
+        arr = None
+        if boxes is not None:
+            arr = np.ascontiguousarray(np.stack([box_floats(b) for b in boxes]), np.float32)
+        return self.L.ref_time_steps(k, delta, None if arr is None else arr.ctypes.data)
+
+    def fields(self) -> dict:
+        n = self.n
+        out = {k: np.empty((n, 4), np.float32) for k in ("position", "velocity", "pressure_accel",
+                                                          "non_pressure_accel", "normal")}
+        out["density"] = np.empty(n, np.float32)
+        out["pressure"] = np.empty(n, np.float32)
+        out["sorted_keys"] = np.empty(n, np.uint64)
+        out["permutation"] = np.empty(n, np.uint32)
+        cnt = np.empty(n, np.uint32)
+        off = np.empty(n, np.uint32)
+        cap = n * 96
+        nbr = np.empty(cap, np.uint32)
+        total = C.c_ulonglong()
+        dt = np.empty(2, np.float32)
+        p = lambda a: a.ctypes.data  # noqa: E731
+        self.L.ref_get_fields(p(out["position"]), p(out["velocity"]), p(out["density"]), p(out["pressure"]),
+                              p(out["pressure_accel"]), p(out["non_pressure_accel"]), p(out["normal"]),
+                              p(out["sorted_keys"]), p(out["permutation"]), p(cnt), p(off), p(nbr), cap,
+                              C.byref(total), p(dt))
+        out["neighbors"] = (cnt, off, nbr[: total.value].copy())
+        out["dt"] = (float(dt[0]), float(dt[1]))
+        T = C.c_uint()
+        self.L.ref_get_hash(None, None, None, C.byref(T))
+        tab = np.empty(T.value, np.uint64)
+        cs = np.empty(T.value, np.uint32)
+        ce = np.empty(T.value, np.uint32)
+        self.L.ref_get_hash(p(tab), p(cs), p(ce), None)
+        out["hash_table"], out["hash_cell_start"], out["hash_cell_end"] = tab, cs, ce
+        if self.nb:
+            bp = np.empty((self.nb, 4), np.float32)
+            bm = np.empty(self.nb, np.float32)
+            self.L.ref_get_boundary(p(bp), p(bm))
+            out["boundary_position"], out["boundary_mass"] = bp, bm
+        return out
+
+    def close(self):
+        self.L.ref_destroy()
+
+
+def bench_line(args, metric: str) -> dict:
+    """`bench.py --impl reference`: the reference CUDA path on the same workload."""
+    sys.path.insert(0, str(HERE.parent / "fluid-simulation_b200"))
+    import wcsph
+
+    variant = args.workload
+    if not available(variant):
+        return {"impl": "reference", "unavailable": f"reference harness for {variant} not built "
+                                                    f"(oracle/build_ref.py needs the reference sources)"}
+    pre = wcsph.preset(args.workload, seed=args.seed)
+    n = pre.info.fluid_n
+    delta = pre.info.delta
+    total = args.warmup + args.steps
+    boxes = [pre.box_at(k + 1) for k in range(total)] if pre.info.moving_box else None
+    sim = RefSim(variant, pre.pos, pre.vel, pre.bpos, pre.box, device=0)
+    sim.time_steps(args.warmup, delta, None if boxes is None else boxes[: args.warmup])
+    t0 = time.perf_counter()
+    ms = sim.time_steps(args.steps, delta, None if boxes is None else boxes[args.warmup:total])
+    wall = time.perf_counter() - t0
+    sim.close()
+    value = n * args.steps / (ms * 1e-3)
+    return {
+        "impl": "reference", "metric": metric, "value": value, "unit": metric, "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (same preset as --impl ours)",
+        "config": {"workload": args.workload, "particles": n, "dt": delta,
+                   "reference_path": "reference kernels (src/cuda/tuning/kernels, frozen config of the "
+                                     "largest shipped scene) + Thrust sort/gather/scan/reduce, host CFL readback"},
+        "cpu_baseline": {"value": value, "unit": metric, "cores": 0, "kind": "reference",
+                         "sample": f"{args.steps} steps of the reference CUDA path (the reference has no CPU solver)"},
+        "e2e": {"value": n * args.steps / wall, "unit": metric, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
