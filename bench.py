@@ -230,6 +230,10 @@ def run_ours(args, world, rank, local, dist):
 
     launches = sim.launches_per_step() * args.steps
     sim.close()
+    extras = {}
+    if world == 1 and not args.no_extras:
+        extras["batched"] = bench_batched(args)
+        extras["rollout"] = bench_rollout()
     if rank != 0:
         return None
     peak, peak_kind = measured_peaks()
@@ -256,9 +260,65 @@ def run_ours(args, world, rank, local, dist):
                      "frac": achieved / peak, "peak_source": peak_kind, "traffic": None,
                      "stage_ms": stage_ms},
     }
+    line.update(extras)
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(pre, args.cpu_budget)
     return line
+
+
+def bench_batched(args, n_scenes: int = 256, steps: int = 20):
+    """Ensemble of 256 scenes (log-uniform 2048..65536 particles): one batched
+    simulator vs the same scenes stepped one after another."""
+    import wcsph
+
+    pres = [wcsph.preset_ensemble(args.seed + 1, k) for k in range(n_scenes)]
+    total = sum(p.info.fluid_n for p in pres)
+    specs = [wcsph.BatchSceneSpec(fluid_pos=s.pos, box=s.box, gravity=tuple(s.params.gravity),
+                                  viscosity=s.params.viscosity, boundary_pos=s.bpos) for s in pres]
+    b = wcsph.BatchSimulator(pres[0].params, specs)
+    b.step_n(3, 1e-3)
+    ms_b = b.time_steps(steps, 1e-3)
+    b.close()
+    sims = [s.simulator() for s in pres]
+    for sim in sims:
+        sim.step_n(3, 1e-3)
+        sim.synchronize()
+    t0 = time.perf_counter()
+    for sim in sims:
+        sim.step_n(steps, 1e-3)
+        sim.synchronize()
+    seq_s = time.perf_counter() - t0
+    for sim in sims:
+        sim.close()
+    vb = total * steps / (ms_b * 1e-3)
+    vs = total * steps / seq_s
+    return {"scenes": n_scenes, "particles": total, "steps": steps, "value": vb, "unit": METRIC,
+            "sequential_value": vs, "gain": vb / vs, "launches_per_step_batched": 14,
+            "launches_per_step_sequential": 14 * n_scenes}
+
+
+def bench_rollout():
+    """Differentiable rollout (16,384 particles, 200 x 1e-3 steps, checkpoints
+    every 20): backward time over forward time."""
+    import wcsph
+
+    pre = wcsph.preset("rollout_block")
+    target = pre.pos.copy()
+    target[:, 0] += 0.2
+    target[:, 2] += 0.1
+    sim = pre.simulator()
+    sim.rollout_forward(20, 1e-3, 20, target)   # warm-up (allocations, module load)
+    sim.rollout_backward()
+    sim.set_state(pre.pos, pre.vel)
+    sim.synchronize()
+    t0 = time.perf_counter()
+    loss = sim.rollout_forward(pre.info.steps, pre.info.delta, 20, target)
+    t1 = time.perf_counter()
+    sim.rollout_backward()
+    t2 = time.perf_counter()
+    sim.close()
+    return {"particles": pre.info.fluid_n, "steps": pre.info.steps, "checkpoint_every": 20, "loss": loss,
+            "forward_ms": (t1 - t0) * 1e3, "backward_ms": (t2 - t1) * 1e3, "backward_over_forward": (t2 - t1) / (t1 - t0)}
 
 
 def run_reference(args, world, rank, local, dist):
@@ -281,6 +341,7 @@ def main():
     ap.add_argument("--workload", default="large_tilting")
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true", help="skip the ensemble and rollout measurements")
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)

@@ -1,3 +1,3 @@
-// batch.cuh — batched ensemble of independent scenes (see batch.cu).
+// batch.cuh — batched ensemble of independent scenes (batch.cu).
 #pragma once
 #include "simulator.cuh"

@@ -55,11 +55,20 @@ void base_params(wcsph_params* p, float r) {
     p->particle_radius = r;
 }
 
-// Benchmark physics shared by the dam-break family: rho0 1000, Tait k 1000,
-// gamma 7, viscosity 0.01, gravity -9.81 y, fixed dt (CFL off).
+// Tait stiffness 1000 in the textbook normalisation of the spiky gradient,
+// -45/(pi h^6) (h - r)^2, expressed in the reference's normalisation
+// -45/(pi h^9) (1 - q)^2 / (h r) (kernel.cuh:43-51), which is h^-6 times
+// stronger: k_ref = 1000 * h^6. A literal k = 1000 with the reference's
+// kernel accelerates particles to ~1e8 m/s in the first step.
+float textbook_stiffness(float k, float r) {
+    return static_cast<float>(static_cast<double>(k) * std::pow(4.0 * static_cast<double>(r), 6.0));
+}
+
+// Benchmark physics shared by the dam-break family: rho0 1000, Tait k 1000
+// (textbook normalisation), gamma 7, viscosity 0.01, gravity -9.81 y, fixed dt.
 void dam_break_physics(wcsph_params* p, float r, float dt) {
     base_params(p, r);
-    p->stiffness = 1000.f;
+    p->stiffness = textbook_stiffness(1000.f, r);
     p->viscosity = 0.01f;
     p->cfl_factor = 0.f;
     p->max_time_step = dt;

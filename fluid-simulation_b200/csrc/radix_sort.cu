@@ -35,7 +35,8 @@ __device__ __forceinline__ void flush_hist(u32 (*s_hist)[256], u32* hist) {
 }  // namespace
 
 __global__ void keys_hist_kernel(const float4* __restrict__ pos, u32 n, float cs,
-                                 u64* __restrict__ keys_out, u32* __restrict__ hist) {
+                                 u64* __restrict__ keys_out, u32* __restrict__ hist,
+                                 const u32* __restrict__ scene) {
     __shared__ u32 s_hist[SORT_DIGITS][256];
     for (int t = threadIdx.x; t < SORT_DIGITS * 256; t += blockDim.x) (&s_hist[0][0])[t] = 0;
     __syncthreads();
@@ -47,6 +48,7 @@ __global__ void keys_hist_kernel(const float4* __restrict__ pos, u32 n, float cs
         u64 key = 0;
         if (valid) {
             key = morton_key(cell_of(pos[i], cs));
+            if (scene) key = batch_key(scene[i], key);
             keys_out[i] = key;
         }
         hist_add_key(s_hist, key, valid);

@@ -123,6 +123,8 @@ CUDASPHSimulator::CUDASPHSimulator(const wcsph_params& params, const wcsph_scene
 }
 
 CUDASPHSimulator::~CUDASPHSimulator() {
+    destroy_adjoint(adjoint_);
+    adjoint_ = nullptr;
     if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
     if (stream_) {
         cudaStreamSynchronize(stream_);
@@ -279,6 +281,22 @@ void CUDASPHSimulator::enqueue_search(bool keys_from_state) {
     launch_reorder_cells(pos_a_.ptr, vel_a_.ptr, vals_[1].ptr, vals_[2].ptr, st_.ptr, n, dp_.cell_size, pos_b_.ptr,
                          vel_b_.ptr, perm_.ptr, ckey_.ptr, table_.ptr, cstart_.ptr, cend_.ptr, table_size_ - 1,
                          st_.ptr, stream_);
+}
+
+TravArgs CUDASPHSimulator::fixed_args(float dt) {
+    TravArgs a = trav_args(dt);
+    a.cfl_factor = 0.f;
+    a.max_dt = dt;
+    a.min_dt = dt;
+    return a;
+}
+
+void CUDASPHSimulator::enqueue_fixed_step(float dt) {
+    enqueue_search(true);
+    const TravArgs a = fixed_args(dt);
+    launch_pass(PASS_DENSITY, dp_, a, stream_, cfg_.warps_density);
+    launch_pass(PASS_FORCE, dp_, a, stream_, cfg_.warps_force);
+    launch_pass(PASS_SURFACE, dp_, a, stream_, cfg_.warps_surface);
 }
 
 void CUDASPHSimulator::enqueue_step(float delta) {

@@ -89,6 +89,7 @@ public:
 };
 
 class Tuner;  // tuner.cuh
+void destroy_adjoint(void* adjoint);  // adjoint.cu
 
 class CUDASPHSimulator final : public FluidSimulator {
 public:
@@ -139,9 +140,12 @@ public:
 
     // Enqueues one step without graph capture (also used inside capture).
     void enqueue_step(float delta);
-    // Enqueues sort + neighbourhood search + density/force passes of one step
-    // on the current state (no integrate); used by parity tools and adjoint.
+    // Enqueues sort + neighbourhood search of one step on the current state.
     void enqueue_search(bool keys_from_state);
+    // Traversal arguments with a fixed time step (CFL off): dt_p = dt.
+    TravArgs fixed_args(float dt);
+    // One step with a fixed time step (the differentiable rollout's forward).
+    void enqueue_fixed_step(float dt);
 
 private:
     void allocate();

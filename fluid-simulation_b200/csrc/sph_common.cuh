@@ -204,10 +204,34 @@ __host__ __device__ __forceinline__ u64 cell_hash_packed(u64 pk) {
                      static_cast<u32>((pk >> 42) & 0x1FFFFFull));
 }
 
+// Batched ensembles key cells by (scene, cell): 16 bits per axis of the offset
+// coordinates plus the scene id in bits 48..62. Scenes must lie inside one
+// 65536-cell window per axis (checked at creation).
+__host__ __device__ __forceinline__ u64 pack_cell_batch(u32 scene, u32 x, u32 y, u32 z) {
+    return (static_cast<u64>(scene) << 48) | static_cast<u64>(x & 0xFFFFu) |
+           (static_cast<u64>(y & 0xFFFFu) << 16) | (static_cast<u64>(z & 0xFFFFu) << 32);
+}
+__host__ __device__ __forceinline__ u64 cell_hash_batch(u64 pk) {
+    const u32 s = static_cast<u32>(pk >> 48);
+    return cell_hash(static_cast<u32>(pk & 0xFFFFull), static_cast<u32>((pk >> 16) & 0xFFFFull),
+                     static_cast<u32>((pk >> 32) & 0xFFFFull)) ^ (0x9E3779B97F4A7C15ull * s);
+}
+template <bool BATCH>
+__host__ __device__ __forceinline__ u64 slot_hash(u64 pk) {
+    if constexpr (BATCH) return cell_hash_batch(pk);
+    else return cell_hash_packed(pk);
+}
+// Sort key of a batched particle: scene in the top bits, the low 48 bits of
+// the reference's Morton key below (identical order inside a scene).
+__host__ __device__ __forceinline__ u64 batch_key(u32 scene, u64 morton) {
+    return (static_cast<u64>(scene) << 48) | (morton & 0xFFFFFFFFFFFFull);
+}
+
 // Linear-probed lookup (find_cell_in_table, common.cuh:89-102). table_size is
 // a power of two so `% T` is a mask; the probe is bounded by T.
+template <bool BATCH = false>
 __device__ __forceinline__ u32 hash_find(const u64* __restrict__ table, u32 tmask, u64 pk) {
-    u32 t = static_cast<u32>(cell_hash_packed(pk) & tmask);
+    u32 t = static_cast<u32>(slot_hash<BATCH>(pk) & tmask);
     for (u32 j = 0; j <= tmask; ++j) {
         const u64 k = __ldg(table + t);
         if (k == EMPTY_HASH) return EMPTY_CELL;
@@ -218,8 +242,9 @@ __device__ __forceinline__ u32 hash_find(const u64* __restrict__ table, u32 tmas
 }
 // add_cell (common.cuh:104-114) with atomicCAS; returns EMPTY_CELL when the
 // table is full (the reference returns -1 and then writes cell_start[-1]).
+template <bool BATCH = false>
 __device__ __forceinline__ u32 hash_insert(u64* table, u32 tmask, u64 pk) {
-    u32 t = static_cast<u32>(cell_hash_packed(pk) & tmask);
+    u32 t = static_cast<u32>(slot_hash<BATCH>(pk) & tmask);
     for (u32 j = 0; j <= tmask; ++j) {
         const u64 old = atomicCAS(table + t, EMPTY_HASH, pk);
         if (old == EMPTY_HASH || old == pk) return t;
@@ -227,6 +252,12 @@ __device__ __forceinline__ u32 hash_insert(u64* table, u32 tmask, u64 pk) {
     }
     return EMPTY_CELL;
 }
+
+// Per-scene constants of a batched ensemble (read by the integrate pass).
+struct DevScene {
+    DevBox box;
+    float4 gravity_visc;   // gravity x, y, z and viscosity * 10 * mass
+};
 
 // Device-side step state: CFL reduction, metrics, sort bookkeeping, errors.
 struct DevState {

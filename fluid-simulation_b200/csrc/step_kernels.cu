@@ -35,7 +35,7 @@ struct WarpSmem {
 
 // Looks up `ncell` cells (lane-parallel) and stores their ranges as
 // (start, exclusive prefix); returns the total candidate count.
-template <class CellFn>
+template <bool BATCH, class CellFn>
 __device__ __forceinline__ u32 gather_ranges(u32* rstart, u32* rpref, u32 ncell, const HashView& hv,
                                              CellFn cell_of_q) {
     const u32 lane = lane_id();
@@ -45,7 +45,7 @@ __device__ __forceinline__ u32 gather_ranges(u32* rstart, u32* rpref, u32 ncell,
         u32 s = 0, cnt = 0;
         if (q < ncell) {
             const u64 pk = cell_of_q(q);
-            const u32 slot = hash_find(hv.table, hv.tmask, pk);
+            const u32 slot = hash_find<BATCH>(hv.table, hv.tmask, pk);
             if (slot != EMPTY_CELL) {
                 s = __ldg(hv.cstart + slot);
                 cnt = __ldg(hv.cend + slot) - s;
@@ -130,21 +130,47 @@ __device__ __forceinline__ float cfl_time_step(const TravArgs& a, const DevParam
 struct HomeData {
     float4 x, v, n, ap, vl;
     float rho, prs, dpi;
+    float4 abar, w;   // adjoint passes
+    float rb;         // dL/drho of the home particle (adjoint density pass)
 };
+
+// d/dr of the coefficient functions (as functions of r = q h):
+//   spiky_grad  g_s = F (1-q)^2 / (h r)            -> -F (1-q)(1+q) / (h r^2)
+//   cubic_grad  g_c = F q (3q-2) / (h r) (q <= .5) -> 3 F / h^3
+//               g_c = -F (1-q)^2 / (h r) (q > .5)   ->  F (1-q)(1+q) / (h r^2)
+__device__ __forceinline__ float spiky_grad_dr(float q, float r, const DevParams& P) {
+    if (q < 1.e-9f || q > 1.f) return 0.f;
+    return -P.spiky_grad_factor * (1.f - q) * (1.f + q) / (P.h * r * r);
+}
+__device__ __forceinline__ float cubic_grad_dr(float q, float r, const DevParams& P) {
+    if (q < 1.e-9f || q > 1.f) return 0.f;
+    if (q <= 0.5f) return 3.f * P.cubic_grad_factor / (P.h * P.h * P.h);
+    return P.cubic_grad_factor * (1.f - q) * (1.f + q) / (P.h * r * r);
+}
 
 template <int KIND>
 __device__ __forceinline__ constexpr bool uses_boundary() {
-    return KIND == PASS_DENSITY || KIND == PASS_FORCE;
+    return KIND == PASS_DENSITY || KIND == PASS_FORCE || KIND == PASS_ADJ_FORCE || KIND == PASS_ADJ_DENSITY;
+}
+template <int KIND>
+__device__ __forceinline__ constexpr bool uses_masks() {
+    return KIND == PASS_FORCE || KIND == PASS_SURFACE || KIND == PASS_ADJ_FORCE || KIND == PASS_ADJ_DENSITY;
 }
 
 // Per-lane accumulators of every pass (unused members are eliminated).
 struct Acc {
     float w;        // density: sum W (fluid), boundary: sum m_b W
     float wb;
-    float4 a;       // pressure accel / surface force
+    float4 a;       // pressure accel (fluid part) / surface force
+    float4 ab;      // boundary pressure accel (added after the fluid mass factor)
     float4 nrm;     // normal
     float4 vl;      // viscosity laplacian
     u32 cnt;
+    // adjoint accumulators
+    float4 xb, vb;  // dL/dx_i, dL/dv_i contributions
+    float pt;       // sum_j -m (abar_i - abar_j) . F(r_ij)   (pressure coefficient sensitivity)
+    float bt;       // sum_b -m_b abar_i . F(r_ib)             (boundary pressure coefficient)
+    float vt;       // sum_j (v_ij . r_ij) G_ij (w_j . r_ij)   (viscosity rho_i sensitivity)
 };
 
 template <int KIND>
@@ -180,6 +206,53 @@ __device__ __forceinline__ void fluid_pair(Acc& acc, const HomeData& H, u32 j, f
             acc.a.y += (P.mass * (r.y / len) * c + H.n.y - nj.y) * inv;
             acc.a.z += (P.mass * (r.z / len) * c + H.n.z - nj.z) * inv;
         }
+    } else if constexpr (KIND == PASS_ADJ_FORCE) {
+        // pressure: a_i = -m sum_j A_ij F(r_ij), F(r) = g_s(|r|) r, A_ij = p_i/rho_i^2 + p_j/rho_j^2
+        const float4 r = f4(H.x.x - xj.x, H.x.y - xj.y, H.x.z - xj.z);
+        const float rl = sqrtf(r2);
+        const float dj = __ldg(a.rho + j);
+        const float pj = __ldg(a.prs + j);
+        const float4 aj = __ldg(a.adj_abar + j);
+        const float gs = spiky_grad(q, P);
+        const float gsp = rl > 0.f ? spiky_grad_dr(q, rl, P) / rl : 0.f;
+        const float A = H.dpi + pj / (dj * dj);
+        const float dax = H.abar.x - aj.x, day = H.abar.y - aj.y, daz = H.abar.z - aj.z;
+        const float rda = r.x * dax + r.y * day + r.z * daz;
+        acc.pt += -P.mass * gs * rda;
+        // x_i: -m A J_F(r) (abar_i - abar_j), J_F = g_s I + (g_s'/|r|) r r^T
+        const float cA = -P.mass * A;
+        acc.xb.x += cA * (gs * dax + gsp * rda * r.x);
+        acc.xb.y += cA * (gs * day + gsp * rda * r.y);
+        acc.xb.z += cA * (gs * daz + gsp * rda * r.z);
+        // viscosity: vlap_i = sum_j (u.r) G(|r|) r / rho_j, u = v_i - v_j, G = g_c / (r^2 + eps)
+        const float4 vj = __ldg(a.vel + j);
+        const float4 wj = __ldg(a.adj_w + j);
+        const float gc = cubic_grad(q, P);
+        const float gcp = rl > 0.f ? cubic_grad_dr(q, rl, P) : 0.f;
+        const float den = r2 + P.visc_eps;
+        const float G = gc / den;
+        const float Gp = rl > 0.f ? (gcp / den - 2.f * rl * gc / (den * den)) / rl : 0.f;  // G'/|r|
+        const float ux = H.v.x - vj.x, uy = H.v.y - vj.y, uz = H.v.z - vj.z;
+        const float ur = ux * r.x + uy * r.y + uz * r.z;
+        const float wir = H.w.x * r.x + H.w.y * r.y + H.w.z * r.z;
+        const float wjr = wj.x * r.x + wj.y * r.y + wj.z * r.z;
+        const float inv_dj = 1.f / dj, inv_di = 1.f / H.rho;
+        const float cv = G * (wir * inv_dj - wjr * inv_di);
+        acc.vb.x += cv * r.x; acc.vb.y += cv * r.y; acc.vb.z += cv * r.z;
+        acc.vt += ur * G * wjr;
+        const float si = inv_dj, sj = inv_di;
+        acc.xb.x += si * (ux * G * wir + ur * G * H.w.x + ur * wir * Gp * r.x) -
+                    sj * (ux * G * wjr + ur * G * wj.x + ur * wjr * Gp * r.x);
+        acc.xb.y += si * (uy * G * wir + ur * G * H.w.y + ur * wir * Gp * r.y) -
+                    sj * (uy * G * wjr + ur * G * wj.y + ur * wjr * Gp * r.y);
+        acc.xb.z += si * (uz * G * wir + ur * G * H.w.z + ur * wir * Gp * r.z) -
+                    sj * (uz * G * wjr + ur * G * wj.z + ur * wjr * Gp * r.z);
+    } else if constexpr (KIND == PASS_ADJ_DENSITY) {
+        // rho_i = m (W(0) + sum_j W(|r_ij|)): dW/dx_i = g_c r_ij, shared by rho_i and rho_j
+        const float rb = __ldg(a.adj_rhobar + j);
+        const float c = P.mass * cubic_grad(q, P) * (H.rb + rb);
+        const float4 r = f4(H.x.x - xj.x, H.x.y - xj.y, H.x.z - xj.z);
+        acc.xb.x += c * r.x; acc.xb.y += c * r.y; acc.xb.z += c * r.z;
     }
 }
 
@@ -193,13 +266,31 @@ __device__ __forceinline__ void boundary_pair(Acc& acc, const HomeData& H, u32 b
     } else if constexpr (KIND == PASS_FORCE) {
         const float b_p_term = H.dpi + H.prs / P.rest_density2;
         const float c = mb * b_p_term * spiky_grad(q, P);
-        acc.a.x -= c * (H.x.x - xb.x);
-        acc.a.y -= c * (H.x.y - xb.y);
-        acc.a.z -= c * (H.x.z - xb.z);
+        acc.ab.x -= c * (H.x.x - xb.x);
+        acc.ab.y -= c * (H.x.y - xb.y);
+        acc.ab.z -= c * (H.x.z - xb.z);
+    } else if constexpr (KIND == PASS_ADJ_FORCE) {
+        // a_i -= m_b B_i F(r_ib), B_i = p_i/rho_i^2 + p_i/rho0^2
+        const float4 r = f4(H.x.x - xb.x, H.x.y - xb.y, H.x.z - xb.z);
+        const float rl = sqrtf(r2);
+        const float gs = spiky_grad(q, P);
+        const float gsp = rl > 0.f ? spiky_grad_dr(q, rl, P) / rl : 0.f;
+        const float B = H.dpi + H.prs / P.rest_density2;
+        const float ra = r.x * H.abar.x + r.y * H.abar.y + r.z * H.abar.z;
+        acc.bt += -mb * gs * ra;
+        const float cB = -mb * B;
+        acc.xb.x += cB * (gs * H.abar.x + gsp * ra * r.x);
+        acc.xb.y += cB * (gs * H.abar.y + gsp * ra * r.y);
+        acc.xb.z += cB * (gs * H.abar.z + gsp * ra * r.z);
+    } else if constexpr (KIND == PASS_ADJ_DENSITY) {
+        const float c = mb * H.rb * cubic_grad(q, P);
+        acc.xb.x += c * (H.x.x - xb.x);
+        acc.xb.y += c * (H.x.y - xb.y);
+        acc.xb.z += c * (H.x.z - xb.z);
     }
 }
 
-template <int KIND, int WPB>
+template <int KIND, int WPB, bool BATCH>
 __global__ void __launch_bounds__(WPB * 32) cell_pass_kernel(const DevParams P, const TravArgs a) {
     __shared__ WarpSmem smem[WPB];
     __shared__ float s_dt, s_np_dt;
@@ -240,15 +331,24 @@ __global__ void __launch_bounds__(WPB * 32) cell_pass_kernel(const DevParams P, 
             const u32 s = __ffs(starts) - 1;
             starts &= starts - 1;
             const u64 pk = __shfl_sync(FULL, my_pk, s);
-            const u32 ux = static_cast<u32>(pk & 0x1FFFFFull);
-            const u32 uy = static_cast<u32>((pk >> 21) & 0x1FFFFFull);
-            const u32 uz = static_cast<u32>((pk >> 42) & 0x1FFFFFull);
+            u32 ux, uy, uz, scene = 0;
+            if constexpr (BATCH) {
+                scene = static_cast<u32>(pk >> 48);
+                ux = static_cast<u32>(pk & 0xFFFFull);
+                uy = static_cast<u32>((pk >> 16) & 0xFFFFull);
+                uz = static_cast<u32>((pk >> 32) & 0xFFFFull);
+            } else {
+                ux = static_cast<u32>(pk & 0x1FFFFFull);
+                uy = static_cast<u32>((pk >> 21) & 0x1FFFFFull);
+                uz = static_cast<u32>((pk >> 42) & 0x1FFFFFull);
+            }
             // fluid neighbour cells in the reference's x, y, z nesting order
-            const u32 M = gather_ranges(S.rstart, S.rpref, ncell, a.fluid, [&](u32 q) {
+            const u32 M = gather_ranges<BATCH>(S.rstart, S.rpref, ncell, a.fluid, [&](u32 q) {
                 const int dz = static_cast<int>(q % D) - R;
                 const int dy = static_cast<int>((q / D) % D) - R;
                 const int dx = static_cast<int>(q / (D * D)) - R;
-                return pack_cell(ux + dx, uy + dy, uz + dz);
+                if constexpr (BATCH) return pack_cell_batch(scene, ux + dx, uy + dy, uz + dz);
+                else return pack_cell(ux + dx, uy + dy, uz + dz);
             });
             const u32 home_start = S.rstart[qc];
             const u32 n_home = S.rpref[qc + 1] - S.rpref[qc];
@@ -279,11 +379,13 @@ __global__ void __launch_bounds__(WPB * 32) cell_pass_kernel(const DevParams P, 
                         if (lane == 0) atomicOr(&a.st->error_flags, ERR_CAND_OVERFLOW);
                         nbc = 0;
                     } else {
-                        MB = gather_ranges(S.bstart, S.bpref, nbc, a.boundary, [&](u32 q) {
+                        MB = gather_ranges<BATCH>(S.bstart, S.bpref, nbc, a.boundary, [&](u32 q) {
                             const int cz = lo[2] + static_cast<int>(q % bz);
                             const int cy = lo[1] + static_cast<int>((q / bz) % by);
                             const int cx = lo[0] + static_cast<int>(q / (bz * by));
-                            return pack_cell(make_int3(cx, cy, cz));
+                            if constexpr (BATCH)
+                                return pack_cell_batch(scene, offset_coord(cx), offset_coord(cy), offset_coord(cz));
+                            else return pack_cell(make_int3(cx, cy, cz));
                         });
                     }
                 }
@@ -313,6 +415,15 @@ __global__ void __launch_bounds__(WPB * 32) cell_pass_kernel(const DevParams P, 
                     H.ap = a.ap[i];
                     H.vl = a.vlap[i];
                 }
+                if constexpr (KIND == PASS_ADJ_FORCE) {
+                    H.v = a.vel[i];
+                    H.rho = a.rho[i];
+                    H.prs = a.prs[i];
+                    H.dpi = H.prs / (H.rho * H.rho);
+                    H.abar = a.adj_abar[i];
+                    H.w = a.adj_w[i];
+                }
+                if constexpr (KIND == PASS_ADJ_DENSITY) H.rb = a.adj_rhobar[i];
                 Acc acc{};
 
                 if constexpr (KIND == PASS_DENSITY) {
@@ -344,7 +455,7 @@ __global__ void __launch_bounds__(WPB * 32) cell_pass_kernel(const DevParams P, 
                             }
                         }
                     }
-                } else if constexpr (KIND == PASS_FORCE || KIND == PASS_SURFACE) {
+                } else if constexpr (uses_masks<KIND>()) {
                     if (masked) {
                         if (hv) {
                             const u32* mrow = a.mask + static_cast<size_t>(i) * a.mask_words;
@@ -422,10 +533,19 @@ __global__ void __launch_bounds__(WPB * 32) cell_pass_kernel(const DevParams P, 
                     acc.wb = group_sum<float>(acc.wb, L);
                 } else if constexpr (KIND == PASS_FORCE) {
                     acc.a = group_sum4(acc.a, L);
+                    acc.ab = group_sum4(acc.ab, L);
                     acc.nrm = group_sum4(acc.nrm, L);
                     acc.vl = group_sum4(acc.vl, L);
                 } else if constexpr (KIND == PASS_SURFACE) {
                     acc.a = group_sum4(acc.a, L);
+                } else if constexpr (KIND == PASS_ADJ_FORCE) {
+                    acc.xb = group_sum4(acc.xb, L);
+                    acc.vb = group_sum4(acc.vb, L);
+                    acc.pt = group_sum<float>(acc.pt, L);
+                    acc.bt = group_sum<float>(acc.bt, L);
+                    acc.vt = group_sum<float>(acc.vt, L);
+                } else if constexpr (KIND == PASS_ADJ_DENSITY) {
+                    acc.xb = group_sum4(acc.xb, L);
                 }
 
                 if (hv && l == 0) {
@@ -435,17 +555,27 @@ __global__ void __launch_bounds__(WPB * 32) cell_pass_kernel(const DevParams P, 
                         a.rho[i] = rho;
                         a.prs[i] = tait_pressure(rho, P);
                     } else if constexpr (KIND == PASS_FORCE) {
-                        a.ap[i] = f4(P.mass * acc.a.x, P.mass * acc.a.y, P.mass * acc.a.z);
+                        // compute_pressure_accel_n_normal_with_boundary: m * sum_fluid, then
+                        // the boundary term (compute_pressure_accel_n_normal.cu:346-364)
+                        a.ap[i] = f4(P.mass * acc.a.x + acc.ab.x, P.mass * acc.a.y + acc.ab.y,
+                                     P.mass * acc.a.z + acc.ab.z);
                         const float sn = P.h * P.mass;
                         a.normal[i] = f4(sn * acc.nrm.x, sn * acc.nrm.y, sn * acc.nrm.z);
                         a.vlap[i] = acc.vl;
                     } else if constexpr (KIND == PASS_SURFACE) {
                         // a_np = g + F_ext + nu*10*m*vlap - alpha*2*rho0*f
                         const float4 fe = external_force(H.x, P);
+                        float4 gv = make_float4(P.gravity[0], P.gravity[1], P.gravity[2], P.visc_scale);
+                        const DevBox* bb = a.box;
+                        if constexpr (BATCH) {
+                            gv = a.scenes[scene].gravity_visc;
+                            bb = &a.scenes[scene].box;
+                            a.scene_state[i] = scene;
+                        }
                         float4 anp;
-                        anp.x = P.gravity[0] + fe.x + P.visc_scale * H.vl.x - P.st_scale * acc.a.x;
-                        anp.y = P.gravity[1] + fe.y + P.visc_scale * H.vl.y - P.st_scale * acc.a.y;
-                        anp.z = P.gravity[2] + fe.z + P.visc_scale * H.vl.z - P.st_scale * acc.a.z;
+                        anp.x = gv.x + fe.x + gv.w * H.vl.x - P.st_scale * acc.a.x;
+                        anp.y = gv.y + fe.y + gv.w * H.vl.y - P.st_scale * acc.a.y;
+                        anp.z = gv.z + fe.z + gv.w * H.vl.z - P.st_scale * acc.a.z;
                         anp.w = 0.f;
                         a.anp[i] = anp;
                         // update_positions.cu:64-67
@@ -457,7 +587,7 @@ __global__ void __launch_bounds__(WPB * 32) cell_pass_kernel(const DevParams P, 
                         x.y += dt * v.y;
                         x.z += dt * v.z;
                         x.w += dt * v.w;
-                        resolve_collision(x, v, *a.box, P);
+                        resolve_collision(x, v, *bb, P);
                         a.pos_out[i] = x;
                         a.vel_out[i] = v;
                         const float s2 = dot3(v, v);
@@ -466,12 +596,34 @@ __global__ void __launch_bounds__(WPB * 32) cell_pass_kernel(const DevParams P, 
                         red_speed2 += s2;
                     } else if constexpr (KIND == PASS_COUNT) {
                         a.counts[i] = acc.cnt;
+                    } else if constexpr (KIND == PASS_ADJ_FORCE) {
+                        const float inv_r2 = 1.f / (H.rho * H.rho);
+                        const float pbar = acc.pt * inv_r2 + acc.bt * (inv_r2 + 1.f / P.rest_density2);
+                        float rhobar = (acc.pt + acc.bt) * (-2.f * H.prs * inv_r2 / H.rho) - acc.vt * inv_r2;
+                        // Tait EOS with the clamp of compute_rho_p.cu:236-238
+                        const float ratio = H.rho / P.rest_density;
+                        const float rc = fminf(fmaxf(ratio, 1.f), P.max_density_ratio);
+                        if (ratio > 1.f && ratio < P.max_density_ratio)
+                            rhobar += pbar * P.stiffness * P.exponent * powf(ratio, P.exponent - 1.f) / P.rest_density;
+                        red_speed += pbar * (powf(rc, P.exponent) - 1.f);  // dL/dk partial
+                        a.adj_rhobar[i] = rhobar;
+                        float4 xb0 = a.adj_xbar[i], vb0 = a.adj_vbar[i];
+                        a.adj_xbar[i] = f4(xb0.x + acc.xb.x, xb0.y + acc.xb.y, xb0.z + acc.xb.z);
+                        a.adj_vbar[i] = f4(vb0.x + acc.vb.x, vb0.y + acc.vb.y, vb0.z + acc.vb.z);
+                    } else if constexpr (KIND == PASS_ADJ_DENSITY) {
+                        float4 xb0 = a.adj_xbar[i];
+                        a.adj_xbar[i] = f4(xb0.x + acc.xb.x, xb0.y + acc.xb.y, xb0.z + acc.xb.z);
                     }
                 }
             }
         }
     }
 
+    if constexpr (KIND == PASS_ADJ_FORCE) {
+        double v = static_cast<double>(red_speed);
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
+        if (lane == 0 && v != 0.0) atomicAdd(a.adj_accum, v);
+    }
     if constexpr (KIND == PASS_SURFACE) {
         // block reduction -> per-block partials (deterministic final sum)
         for (int o = 16; o > 0; o >>= 1) {
@@ -523,12 +675,20 @@ __global__ void __launch_bounds__(WPB * 32) cell_pass_kernel(const DevParams P, 
     }
 }
 
+template <bool BATCH>
+__device__ __forceinline__ u64 cell_key_of(float4 p, float cs, const u32* scene_in, u32 src) {
+    const int3 c = cell_of(p, cs);
+    if constexpr (BATCH) return pack_cell_batch(scene_in[src], offset_coord(c.x), offset_coord(c.y), offset_coord(c.z));
+    else return pack_cell(c);
+}
+
+template <bool BATCH>
 __global__ void reorder_cells_kernel(const float4* __restrict__ pos_in, const float4* __restrict__ vel_in,
                                      const u32* __restrict__ v1, const u32* __restrict__ v2,
                                      const DevState* st, u32 n, float cs, float4* __restrict__ pos_out,
                                      float4* __restrict__ vel_out, u32* __restrict__ perm_out,
                                      u64* __restrict__ ckey_out, u64* table, u32* cstart, u32* cend,
-                                     u32 tmask, DevState* st_err) {
+                                     u32 tmask, DevState* st_err, const u32* __restrict__ scene_in) {
     const u32 i = blockIdx.x * blockDim.x + threadIdx.x;
     const u32 lane = threadIdx.x & 31u;
     const u32 sel = st->sort_sel[8];
@@ -541,23 +701,29 @@ __global__ void reorder_cells_kernel(const float4* __restrict__ pos_in, const fl
         pos_out[i] = p;
         if (vel_out) vel_out[i] = vel_in[src];
         perm_out[i] = src;
-        pk = pack_cell(cell_of(p, cs));
+        pk = cell_key_of<BATCH>(p, cs, scene_in, src);
         ckey_out[i] = pk;
     }
     u64 prev = __shfl_up_sync(FULL, pk, 1);
     u64 next = __shfl_down_sync(FULL, pk, 1);
-    if (valid && lane == 0 && i > 0) prev = pack_cell(cell_of(pos_in[perm ? perm[i - 1] : i - 1], cs));
-    if (valid && lane == 31 && i + 1 < n) next = pack_cell(cell_of(pos_in[perm ? perm[i + 1] : i + 1], cs));
+    if (valid && lane == 0 && i > 0) {
+        const u32 s2 = perm ? perm[i - 1] : i - 1;
+        prev = cell_key_of<BATCH>(pos_in[s2], cs, scene_in, s2);
+    }
+    if (valid && lane == 31 && i + 1 < n) {
+        const u32 s2 = perm ? perm[i + 1] : i + 1;
+        next = cell_key_of<BATCH>(pos_in[s2], cs, scene_in, s2);
+    }
     if (!valid) return;
     // rebuild_n_search.cu:19-34: a run of equal cells starts where the key
     // changes and ends (non-inclusive) at the next change.
     if (i == 0 || pk != prev) {
-        const u32 slot = hash_insert(table, tmask, pk);
+        const u32 slot = hash_insert<BATCH>(table, tmask, pk);
         if (slot == EMPTY_CELL) atomicOr(&st_err->error_flags, ERR_HASH_FULL);
         else cstart[slot] = i;
     }
     if (i == n - 1 || pk != next) {
-        const u32 slot = hash_insert(table, tmask, pk);
+        const u32 slot = hash_insert<BATCH>(table, tmask, pk);
         if (slot == EMPTY_CELL) atomicOr(&st_err->error_flags, ERR_HASH_FULL);
         else cend[slot] = i + 1;
     }
@@ -597,18 +763,24 @@ __global__ void metrics_kernel(const float4* __restrict__ vel, u32 n, float mass
     }
 }
 
+template <bool BATCH>
 __global__ void boundary_mass_kernel(const DevParams P, const float4* __restrict__ bpos, u32 nb, HashView bh,
-                                     float* __restrict__ bmass) {
+                                     float* __restrict__ bmass, const u64* __restrict__ bckey) {
     const u32 i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nb) return;
     const float4 xi = bpos[i];
     const int3 c = cell_of(xi, P.h);
+    const u32 scene = BATCH ? static_cast<u32>(bckey[i] >> 48) : 0u;
     float sum = P.w0;  // cubic_spline(0, h)
     for (int x = -1; x <= 1; ++x)
         for (int y = -1; y <= 1; ++y)
             for (int z = -1; z <= 1; ++z) {
-                const u64 pk = pack_cell(offset_coord(c.x) + x, offset_coord(c.y) + y, offset_coord(c.z) + z);
-                const u32 slot = hash_find(bh.table, bh.tmask, pk);
+                u64 pk;
+                if constexpr (BATCH)
+                    pk = pack_cell_batch(scene, offset_coord(c.x) + x, offset_coord(c.y) + y, offset_coord(c.z) + z);
+                else
+                    pk = pack_cell(offset_coord(c.x) + x, offset_coord(c.y) + y, offset_coord(c.z) + z);
+                const u32 slot = hash_find<BATCH>(bh.table, bh.tmask, pk);
                 if (slot == EMPTY_CELL) continue;
                 const u32 s = bh.cstart[slot], e = bh.cend[slot];
                 for (u32 j = s; j < e; ++j) {
@@ -630,35 +802,49 @@ u32 pass_grid(u32 n, int wpb) {
 void launch_reorder_cells(const float4* pos_in, const float4* vel_in, const u32* perm_src1, const u32* perm_src2,
                           const DevState* st, u32 n, float cs, float4* pos_out, float4* vel_out, u32* perm_out,
                           u64* ckey_out, u64* table, u32* cstart, u32* cend, u32 tmask, DevState* st_err,
-                          cudaStream_t stream) {
+                          cudaStream_t stream, const u32* scene_in) {
     if (n == 0) return;
     const u32 threads = 256;
-    reorder_cells_kernel<<<(n + threads - 1) / threads, threads, 0, stream>>>(
-        pos_in, vel_in, perm_src1, perm_src2, st, n, cs, pos_out, vel_out, perm_out, ckey_out, table, cstart,
-        cend, tmask, st_err);
+    const u32 grid = (n + threads - 1) / threads;
+    if (scene_in)
+        reorder_cells_kernel<true><<<grid, threads, 0, stream>>>(pos_in, vel_in, perm_src1, perm_src2, st, n, cs,
+                                                                 pos_out, vel_out, perm_out, ckey_out, table, cstart,
+                                                                 cend, tmask, st_err, scene_in);
+    else
+        reorder_cells_kernel<false><<<grid, threads, 0, stream>>>(pos_in, vel_in, perm_src1, perm_src2, st, n, cs,
+                                                                  pos_out, vel_out, perm_out, ckey_out, table, cstart,
+                                                                  cend, tmask, st_err, nullptr);
 }
 
-template <int KIND>
+template <int KIND, bool BATCH>
 static void launch_kind(const DevParams& P, const TravArgs& a, cudaStream_t stream, int wpb) {
     const u32 grid = pass_grid(a.n, wpb);
     if (grid == 0) return;
     switch (wpb) {
-    case 2: cell_pass_kernel<KIND, 2><<<grid, 64, 0, stream>>>(P, a); break;
-    case 8: cell_pass_kernel<KIND, 8><<<grid, 256, 0, stream>>>(P, a); break;
-    default: cell_pass_kernel<KIND, 4><<<grid, 128, 0, stream>>>(P, a); break;
+    case 2: cell_pass_kernel<KIND, 2, BATCH><<<grid, 64, 0, stream>>>(P, a); break;
+    case 8: cell_pass_kernel<KIND, 8, BATCH><<<grid, 256, 0, stream>>>(P, a); break;
+    default: cell_pass_kernel<KIND, 4, BATCH><<<grid, 128, 0, stream>>>(P, a); break;
     }
 }
 
-void launch_pass(int kind, const DevParams& P, const TravArgs& a, cudaStream_t stream, int wpb) {
-    if (wpb != 2 && wpb != 8) wpb = 4;
+template <bool BATCH>
+static void launch_pass_t(int kind, const DevParams& P, const TravArgs& a, cudaStream_t stream, int wpb) {
     switch (kind) {
-    case PASS_DENSITY: launch_kind<PASS_DENSITY>(P, a, stream, wpb); break;
-    case PASS_FORCE: launch_kind<PASS_FORCE>(P, a, stream, wpb); break;
-    case PASS_SURFACE: launch_kind<PASS_SURFACE>(P, a, stream, wpb); break;
-    case PASS_COUNT: launch_kind<PASS_COUNT>(P, a, stream, wpb); break;
-    case PASS_FILL: launch_kind<PASS_FILL>(P, a, stream, wpb); break;
+    case PASS_DENSITY: launch_kind<PASS_DENSITY, BATCH>(P, a, stream, wpb); break;
+    case PASS_FORCE: launch_kind<PASS_FORCE, BATCH>(P, a, stream, wpb); break;
+    case PASS_SURFACE: launch_kind<PASS_SURFACE, BATCH>(P, a, stream, wpb); break;
+    case PASS_COUNT: launch_kind<PASS_COUNT, BATCH>(P, a, stream, wpb); break;
+    case PASS_FILL: launch_kind<PASS_FILL, BATCH>(P, a, stream, wpb); break;
+    case PASS_ADJ_FORCE: launch_kind<PASS_ADJ_FORCE, BATCH>(P, a, stream, wpb); break;
+    case PASS_ADJ_DENSITY: launch_kind<PASS_ADJ_DENSITY, BATCH>(P, a, stream, wpb); break;
     default: break;
     }
+}
+
+void launch_pass(int kind, const DevParams& P, const TravArgs& a, cudaStream_t stream, int wpb, bool batch) {
+    if (wpb != 2 && wpb != 8) wpb = 4;
+    if (batch) launch_pass_t<true>(kind, P, a, stream, wpb);
+    else launch_pass_t<false>(kind, P, a, stream, wpb);
 }
 
 void launch_init_cfl(const float4* vel, u32 n, DevState* st, cudaStream_t stream) {
@@ -668,9 +854,10 @@ void launch_init_cfl(const float4* vel, u32 n, DevState* st, cudaStream_t stream
 }
 
 void launch_boundary_mass(const DevParams& P, const float4* bpos, u32 nb, HashView bh, float* bmass,
-                          cudaStream_t stream) {
+                          cudaStream_t stream, const u64* bckey) {
     if (nb == 0) return;
-    boundary_mass_kernel<<<(nb + 127) / 128, 128, 0, stream>>>(P, bpos, nb, bh, bmass);
+    if (bckey) boundary_mass_kernel<true><<<(nb + 127) / 128, 128, 0, stream>>>(P, bpos, nb, bh, bmass, bckey);
+    else boundary_mass_kernel<false><<<(nb + 127) / 128, 128, 0, stream>>>(P, bpos, nb, bh, bmass, nullptr);
 }
 
 void launch_metrics(const float4* vel, u32 n, float mass, float* out2, cudaStream_t stream) {

@@ -63,33 +63,50 @@ struct TravArgs {
     float4* pos_out;
     float4* vel_out;
     DevBox* box;              // device copy of the collision box
+    const DevScene* scenes;   // batched ensembles: per-scene box, gravity, viscosity
+    u32* scene_state;         // batched ensembles: scene id of each state particle (written by the integrate pass)
     DevState* st;
     float delta;              // requested step (host value)
     float cfl_factor;
     float max_dt, min_dt, np_max_dt;
     float metric_mass;        // host-side PARTICLE_MASS used by the ke metric
     float* block_partials;    // [gridDim.x][2] sum|v|, sum|v|^2
+    // adjoint passes (differentiable rollout)
+    const float4* adj_abar;   // dL/da_p per sorted particle
+    const float4* adj_w;      // dL/d(vlap) = nu*10*m * dL/da_np
+    float4* adj_xbar;         // dL/dx (sorted), accumulated
+    float4* adj_vbar;         // dL/dv (sorted), accumulated
+    float* adj_rhobar;        // dL/drho (complete after the adjoint force pass)
+    double* adj_accum;        // [0] dL/dk
     u32* counts;              // neighbour export: counts
     const u32* offsets;       // neighbour export: offsets
     u32* nbr_out;             // neighbour export: indices
     unsigned long long nbr_capacity;
 };
 
-enum PassKind : int { PASS_DENSITY = 0, PASS_FORCE = 1, PASS_SURFACE = 2, PASS_COUNT = 3, PASS_FILL = 4 };
+enum PassKind : int {
+    PASS_DENSITY = 0, PASS_FORCE = 1, PASS_SURFACE = 2, PASS_COUNT = 3, PASS_FILL = 4,
+    PASS_ADJ_FORCE = 5,    // reverse of pressure force (+boundary), viscosity and the Tait EOS
+    PASS_ADJ_DENSITY = 6   // reverse of the density sum (+boundary)
+};
 
+// scene_in != nullptr selects the batched (scene, cell) keys.
 void launch_reorder_cells(const float4* pos_in, const float4* vel_in, const u32* perm_src1,
                           const u32* perm_src2, const DevState* st, u32 n, float cs, float4* pos_out,
                           float4* vel_out, u32* perm_out, u64* ckey_out, u64* table, u32* cstart,
-                          u32* cend, u32 tmask, DevState* st_err, cudaStream_t stream);
+                          u32* cend, u32 tmask, DevState* st_err, cudaStream_t stream,
+                          const u32* scene_in = nullptr);
 
-void launch_pass(int kind, const DevParams& P, const TravArgs& a, cudaStream_t stream, int warps_per_block);
+void launch_pass(int kind, const DevParams& P, const TravArgs& a, cudaStream_t stream, int warps_per_block,
+                 bool batch = false);
 u32 pass_grid(u32 n, int warps_per_block);
 
 // CFL max |v|^2 of a velocity array into st->vmax2_bits[st->parity].
 void launch_init_cfl(const float4* vel, u32 n, DevState* st, cudaStream_t stream);
 // Boundary masses (compute_boundary_mass.cu:10-30), per-thread, init only.
+// bckey != nullptr (batched): packed (scene, cell) key of each sorted boundary particle.
 void launch_boundary_mass(const DevParams& P, const float4* bpos, u32 nb, HashView bh, float* bmass,
-                          cudaStream_t stream);
+                          cudaStream_t stream, const u64* bckey = nullptr);
 // Metrics of an arbitrary velocity array (used after load/reset).
 void launch_metrics(const float4* vel, u32 n, float mass, float* out2, cudaStream_t stream);
 

@@ -537,6 +537,19 @@ class CUDASPHSimulator:
         return gv, gnu.value, gk.value
 
 
+def shard_scenes(counts, world: int) -> list[list[int]]:
+    """Greedy longest-processing-time bin packing of independent scenes onto
+    `world` ranks by particle count (the ensemble shards with no data-path
+    collective). Deterministic: ties go to the lowest rank."""
+    loads = [0] * world
+    shards: list[list[int]] = [[] for _ in range(world)]
+    for k in sorted(range(len(counts)), key=lambda i: (-int(counts[i]), i)):
+        r = min(range(world), key=lambda q: (loads[q], q))
+        shards[r].append(k)
+        loads[r] += int(counts[k])
+    return [sorted(s) for s in shards]
+
+
 @dataclass
 class BatchSceneSpec:
     fluid_pos: np.ndarray

@@ -45,16 +45,24 @@ VARIANTS = {
     # 1,048,576-particle tilting box; frozen config of the largest shipped
     # scene (measurements/configs/BIG_falling.json: all blocks 32,
     # TABLE_SIZE_MULT 4, CELL_SIZE_MULT 1.0, neighbour lists, no smem)
-    "large_tilting": dict(n=1048576, nb=0, r=0.004, k=1000.0, nu=0.01, max_dt=5e-4, cfl=0.0, table_mult=4, block=32),
+    "large_tilting": dict(n=1048576, nb=0, r=0.004, k=("textbook", 1000.0), nu=0.01, max_dt=5e-4, cfl=0.0, table_mult=4, block=32),
     # 32^3 dam break with walls (dragon_settled.json: blocks 32, TABLE_SIZE_MULT 32)
-    "dam_break": dict(n=32768, nb=7802, r=0.01, k=1000.0, nu=0.01, max_dt=1e-3, cfl=0.0, table_mult=32, block=32),
+    "dam_break": dict(n=32768, nb=7802, r=0.01, k=("textbook", 1000.0), nu=0.01, max_dt=1e-3, cfl=0.0, table_mult=32, block=32),
     # golden fixtures (2048 particles)
     "fixture_surface": dict(n=2048, nb=0, force="([](float4 pos) { return make_float4(0., 9.81f, 0., 0.); })",
                             table_mult=8, block=64),
     "fixture_tilting": dict(n=2048, nb=0, table_mult=16, block=32),
-    "fixture_dambreak": dict(n=2048, nb=3202, r=0.01, k=1000.0, nu=0.01, max_dt=1e-3, cfl=0.0, table_mult=4,
+    "fixture_dambreak": dict(n=2048, nb=3202, r=0.01, k=("textbook", 1000.0), nu=0.01, max_dt=1e-3, cfl=0.0, table_mult=4,
                              block=32),
 }
+
+
+def textbook_stiffness(k: float, r: float) -> float:
+    """k * h^6 with h = 4r (float32 of the double product, as the presets compute it)."""
+    import numpy as np
+
+    rd = float(np.float32(r))
+    return float(np.float32(k * (4.0 * rd) ** 6))
 
 
 def bit_ceil(x: int) -> int:
@@ -105,11 +113,13 @@ def shim_sources(ref: Path, dst: Path):
 def variant_config(spec: dict) -> str:
     v = dict(REF_DEFAULT)
     v.update(spec)
+    if isinstance(v["k"], tuple):
+        v["k"] = textbook_stiffness(v["k"][1], v["r"])
     n, nb = v["n"], v["nb"]
     lines = [
         "#pragma once",
         f"#define REF_PARTICLE_RADIUS {v['r']!r}f",
-        f"#define REF_STIFFNESS {v['k']!r}f",
+        f"#define REF_STIFFNESS {v['k']:.9g}f",
         f"#define REF_VISCOSITY {v['nu']!r}f",
         f"#define REF_SURFACE_TENSION {v['alpha']!r}f",
         f"#define REF_GX {v['g'][0]!r}f",

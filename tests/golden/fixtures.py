@@ -18,6 +18,12 @@ NAMES = ("fixture_surface", "fixture_tilting", "fixture_dambreak")
 DAMBREAK_TANK = (0.6, 0.4, 0.4)
 
 
+def textbook_stiffness(k: float, r: float) -> float:
+    """Tait k in the textbook spiky normalisation -> the reference's (k * (4r)^6)."""
+    rd = float(np.float32(r))
+    return float(np.float32(k * (4.0 * rd) ** 6))
+
+
 def scene(name: str):
     """-> (params, box, pos, vel, boundary_pos or None, delta)."""
     if name == "fixture_surface":
@@ -34,8 +40,8 @@ def scene(name: str):
         return p, bx, pos, vel, None, 0.01
     if name == "fixture_dambreak":
         r = 0.01
-        p = wcsph.default_params(particle_radius=r, stiffness=1000.0, viscosity=0.01, max_time_step=1e-3,
-                                 cfl_factor=0.0, table_size_mult=4)
+        p = wcsph.default_params(particle_radius=r, stiffness=textbook_stiffness(1000.0, r), viscosity=0.01,
+                                 max_time_step=1e-3, cfl_factor=0.0, table_size_mult=4)
         dims = (16, 16, 8)
         pos = wcsph.make_lattice(tuple(r + (d - 1) * r for d in dims), dims, r, 0.1 * r, 7)
         bpos = wcsph.sample_box_walls((0, 0, 0), DAMBREAK_TANK, 2 * r)

@@ -21,11 +21,23 @@ sys.path.insert(0, str(HERE))
 sys.path.insert(0, str(ROOT / "oracle"))
 
 
-def one(name: str, out_dir: Path):
+def scene_of(name: str):
+    """Fixture scenes, or any preset workload with a harness variant of its name."""
     import fixtures
+
+    if name in fixtures.NAMES:
+        return fixtures.scene(name)
+    sys.path.insert(0, str(ROOT / "fluid-simulation_b200"))
+    import wcsph
+
+    pre = wcsph.preset(name)
+    return pre.params, pre.box, pre.pos, pre.vel, pre.bpos, pre.info.delta
+
+
+def one(name: str, out_dir: Path):
     import refpath
 
-    p, bx, pos, vel, bpos, delta = fixtures.scene(name)
+    p, bx, pos, vel, bpos, delta = scene_of(name)
     sim = refpath.RefSim(name, pos, vel, bpos, bx)
     sim.step(delta)
     f = sim.fields()
@@ -41,9 +53,10 @@ def one(name: str, out_dir: Path):
 
 
 def main():
-    out = Path(sys.argv[1]) if len(sys.argv) > 1 and not sys.argv[1].startswith("fixture") else HERE
-    if len(sys.argv) > 1 and sys.argv[-1].startswith("fixture"):
-        one(sys.argv[-1], out)
+    # make_ref_fixtures.py [out_dir [scene]]
+    out = Path(sys.argv[1]) if len(sys.argv) > 1 else HERE
+    if len(sys.argv) > 2:
+        one(sys.argv[2], out)
         return
     import fixtures
     for name in fixtures.NAMES:

@@ -106,7 +106,9 @@ def test_icosphere_surface_sampling():
 def test_presets_match_the_workloads():
     d = wcsph.preset("dam_break")
     assert (d.info.fluid_n, d.info.boundary_n, d.info.steps) == (32768, 7802, 1000)
-    assert np.float32(d.params.stiffness) == 1000 and np.float32(d.params.viscosity) == np.float32(0.01)
+    # Tait k = 1000 in the textbook spiky normalisation = 1000 h^6 in the reference's
+    assert np.float32(d.params.stiffness) == np.float32(1000.0 * (4.0 * float(np.float32(0.01))) ** 6)
+    assert np.float32(d.params.viscosity) == np.float32(0.01)
     assert d.params.cfl_factor == 0 and np.float32(d.params.max_time_step) == np.float32(1e-3)
     t = wcsph.preset("large_tilting")
     assert t.info.fluid_n == 1048576 and t.info.boundary_n == 0 and t.info.moving_box == 1
