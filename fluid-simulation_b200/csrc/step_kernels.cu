@@ -9,8 +9,9 @@ namespace wcsph {
 namespace {
 
 constexpr u32 FULL = 0xffffffffu;
-constexpr int CAND_CAP = 512;        // fluid candidates staged per warp (= 32 * max mask words)
-constexpr int BCAND_CAP = 256;       // boundary candidates staged per warp and chunk
+constexpr u32 BCAND_CAP = 256;   // boundary candidates expanded per warp and chunk
+constexpr u32 HOME_BLOCK = 32;   // home particles (bit-matrix rows) handled together
+constexpr u32 SEG_SLOTS = 64;    // segment partials, slot = lane + row (both < 32)
 
 __device__ __forceinline__ u32 lane_id() { return threadIdx.x & 31u; }
 
@@ -24,14 +25,78 @@ __device__ __forceinline__ u32 warp_incl_scan(u32 v) {
     return v;
 }
 
-struct WarpSmem {
-    u32 cand[CAND_CAP];
-    u32 rstart[MAX_RANGE_CELLS + 3];
-    u32 rpref[MAX_RANGE_CELLS + 3];
-    u32 bcand[BCAND_CAP];
-    u32 bstart[MAX_BOUNDARY_CELLS + 3];
-    u32 bpref[MAX_BOUNDARY_CELLS + 3];
+// What each pass stages per candidate and how many floats it accumulates
+// per (home, candidate-run) segment.
+//   sa: DENSITY / COUNT / FILL / ADJ_*: position
+//       FORCE:   (x, y, z, p_j / rho_j^2)    sb = (v_j, 1 / rho_j)
+//       SURFACE: (x, y, z, rho_j)            sb = (n_j, 0)
+//   cand: particle index of the candidate (passes that address j directly)
+template <int KIND>
+struct KindCfg {
+    static constexpr bool stage_b = KIND == PASS_FORCE || KIND == PASS_SURFACE;
+    static constexpr bool stage_j =
+        KIND == PASS_COUNT || KIND == PASS_FILL || KIND == PASS_ADJ_FORCE || KIND == PASS_ADJ_DENSITY;
+    static constexpr bool boundary =
+        KIND == PASS_DENSITY || KIND == PASS_FORCE || KIND == PASS_ADJ_FORCE || KIND == PASS_ADJ_DENSITY;
+    static constexpr int nf = (KIND == PASS_FORCE || KIND == PASS_ADJ_FORCE) ? 9
+                              : (KIND == PASS_SURFACE || KIND == PASS_ADJ_DENSITY) ? 3 : 1;
+    static constexpr int nfb = KIND == PASS_ADJ_FORCE ? 4 : (KIND == PASS_DENSITY ? 1 : 3);
 };
+
+__host__ __device__ constexpr size_t align16(size_t b) { return (b + 15) & ~static_cast<size_t>(15); }
+
+// Per-warp shared memory, sized by the candidate capacity cap = 32 * mask_words.
+template <int KIND>
+struct WarpView {
+    float4* sa;
+    float4* sb;
+    u32* cand;
+    u32* rstart;   // fluid cells: first particle
+    u32* rpref;    // fluid cells: exclusive prefix of the cell sizes (+ total)
+    u32* bcand;
+    u32* bstart;
+    u32* bpref;
+    float* part;   // [SEG_SLOTS][nf] segment partials
+    u32* aux;      // density: the block's bit matrix (cap words); others: row hit offsets
+};
+
+template <int KIND>
+__host__ __device__ __forceinline__ size_t warp_smem_bytes(u32 cap, WarpView<KIND>* v = nullptr,
+                                                           unsigned char* base = nullptr) {
+    using C = KindCfg<KIND>;
+    size_t o = 0;
+    auto take = [&](size_t bytes) {
+        unsigned char* p = base ? base + o : nullptr;
+        o += align16(bytes);
+        return p;
+    };
+    unsigned char* sa = take(16ull * cap);
+    unsigned char* sb = C::stage_b ? take(16ull * cap) : nullptr;
+    unsigned char* cand = C::stage_j ? take(4ull * cap) : nullptr;
+    unsigned char* rstart = take(4ull * (MAX_RANGE_CELLS + 3));
+    unsigned char* rpref = take(4ull * (MAX_RANGE_CELLS + 3));
+    unsigned char *bcand = nullptr, *bstart = nullptr, *bpref = nullptr;
+    if (C::boundary) {
+        bcand = take(4ull * BCAND_CAP);
+        bstart = take(4ull * (MAX_BOUNDARY_CELLS + 3));
+        bpref = take(4ull * (MAX_BOUNDARY_CELLS + 3));
+    }
+    unsigned char* part = take(4ull * SEG_SLOTS * C::nf);
+    unsigned char* aux = take(KIND == PASS_DENSITY ? 4ull * cap : 4ull * (HOME_BLOCK + 4));
+    if (v) {
+        v->sa = reinterpret_cast<float4*>(sa);
+        v->sb = reinterpret_cast<float4*>(sb);
+        v->cand = reinterpret_cast<u32*>(cand);
+        v->rstart = reinterpret_cast<u32*>(rstart);
+        v->rpref = reinterpret_cast<u32*>(rpref);
+        v->bcand = reinterpret_cast<u32*>(bcand);
+        v->bstart = reinterpret_cast<u32*>(bstart);
+        v->bpref = reinterpret_cast<u32*>(bpref);
+        v->part = reinterpret_cast<float*>(part);
+        v->aux = reinterpret_cast<u32*>(aux);
+    }
+    return o;
+}
 
 // Looks up `ncell` cells (lane-parallel) and stores their ranges as
 // (start, exclusive prefix); returns the total candidate count.
@@ -63,37 +128,55 @@ __device__ __forceinline__ u32 gather_ranges(u32* rstart, u32* rpref, u32 ncell,
     return total;
 }
 
+// Index of the range holding candidate m (rpref[lo] <= m < rpref[lo + 1]).
+__device__ __forceinline__ u32 range_of(const u32* rpref, u32 ncell, u32 m) {
+    u32 lo = 0, hi = ncell;
+    while (hi - lo > 1) {
+        const u32 mid = (lo + hi) >> 1;
+        if (rpref[mid] <= m) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
 // cand[m - c0] = particle index of candidate m, m in [c0, c0 + len).
-__device__ __forceinline__ void expand(u32* cand, const u32* rstart, const u32* rpref, u32 ncell,
-                                       u32 c0, u32 len) {
+__device__ __forceinline__ void expand(u32* cand, const u32* rstart, const u32* rpref, u32 ncell, u32 c0,
+                                       u32 len) {
     __syncwarp();
     for (u32 ml = lane_id(); ml < len; ml += 32) {
         const u32 m = c0 + ml;
-        u32 lo = 0, hi = ncell;
-        while (hi - lo > 1) {
-            const u32 mid = (lo + hi) >> 1;
-            if (rpref[mid] <= m) lo = mid; else hi = mid;
-        }
+        const u32 lo = range_of(rpref, ncell, m);
         cand[ml] = rstart[lo] + (m - rpref[lo]);
     }
     __syncwarp();
 }
 
-template <typename T>
-__device__ __forceinline__ T group_sum(T v, u32 L);
-
-template <>
-__device__ __forceinline__ float group_sum<float>(float v, u32 L) {
-    for (u32 o = L >> 1; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
-    return v;
-}
-__device__ __forceinline__ float4 group_sum4(float4 v, u32 L) {
-    for (u32 o = L >> 1; o > 0; o >>= 1) {
-        v.x += __shfl_xor_sync(FULL, v.x, o);
-        v.y += __shfl_xor_sync(FULL, v.y, o);
-        v.z += __shfl_xor_sync(FULL, v.z, o);
+// Like expand(), and stages the candidates' fields into shared memory with
+// lane-parallel loads (the pair loops then read shared memory only).
+template <int KIND>
+__device__ __forceinline__ void stage(const WarpView<KIND>& S, const TravArgs& a, u32 ncell, u32 c0, u32 len) {
+    __syncwarp();
+    for (u32 ml = lane_id(); ml < len; ml += 32) {
+        const u32 m = c0 + ml;
+        const u32 lo = range_of(S.rpref, ncell, m);
+        const u32 j = S.rstart[lo] + (m - S.rpref[lo]);
+        if constexpr (KindCfg<KIND>::stage_j) S.cand[ml] = j;
+        const float4 x = __ldg(a.pos + j);
+        if constexpr (KIND == PASS_FORCE) {
+            const float dj = __ldg(a.rho + j);
+            const float pj = __ldg(a.prs + j);
+            const float4 v = __ldg(a.vel + j);
+            S.sa[ml] = make_float4(x.x, x.y, x.z, pj / (dj * dj));
+            S.sb[ml] = make_float4(v.x, v.y, v.z, 1.f / dj);
+        } else if constexpr (KIND == PASS_SURFACE) {
+            const float dj = __ldg(a.rho + j);
+            const float4 nj = __ldg(a.normal + j);
+            S.sa[ml] = make_float4(x.x, x.y, x.z, dj);
+            S.sb[ml] = make_float4(nj.x, nj.y, nj.z, 0.f);
+        } else {
+            S.sa[ml] = x;
+        }
     }
-    return v;
+    __syncwarp();
 }
 
 __device__ __forceinline__ float4 f4(float x, float y, float z, float w = 0.f) { return make_float4(x, y, z, w); }
@@ -128,11 +211,32 @@ __device__ __forceinline__ float cfl_time_step(const TravArgs& a, const DevParam
 }
 
 struct HomeData {
-    float4 x, v, n, ap, vl;
+    float4 x, v, n, abar, w;
     float rho, prs, dpi;
-    float4 abar, w;   // adjoint passes
     float rb;         // dL/drho of the home particle (adjoint density pass)
 };
+
+template <int KIND>
+__device__ __forceinline__ HomeData load_home(const TravArgs& a, u32 i) {
+    HomeData H;
+    H.x = __ldg(a.pos + i);
+    if constexpr (KIND == PASS_FORCE || KIND == PASS_ADJ_FORCE) {
+        H.v = __ldg(a.vel + i);
+        H.rho = __ldg(a.rho + i);
+        H.prs = __ldg(a.prs + i);
+        H.dpi = H.prs / (H.rho * H.rho);
+    }
+    if constexpr (KIND == PASS_SURFACE) {
+        H.rho = __ldg(a.rho + i);
+        H.n = __ldg(a.normal + i);
+    }
+    if constexpr (KIND == PASS_ADJ_FORCE) {
+        H.abar = __ldg(a.adj_abar + i);
+        H.w = __ldg(a.adj_w + i);
+    }
+    if constexpr (KIND == PASS_ADJ_DENSITY) H.rb = __ldg(a.adj_rhobar + i);
+    return H;
+}
 
 // d/dr of the coefficient functions (as functions of r = q h):
 //   spiky_grad  g_s = F (1-q)^2 / (h r)            -> -F (1-q)(1+q) / (h r^2)
@@ -148,68 +252,67 @@ __device__ __forceinline__ float cubic_grad_dr(float q, float r, const DevParams
     return P.cubic_grad_factor * (1.f - q) * (1.f + q) / (P.h * r * r);
 }
 
-template <int KIND>
-__device__ __forceinline__ constexpr bool uses_boundary() {
-    return KIND == PASS_DENSITY || KIND == PASS_FORCE || KIND == PASS_ADJ_FORCE || KIND == PASS_ADJ_DENSITY;
-}
-template <int KIND>
-__device__ __forceinline__ constexpr bool uses_masks() {
-    return KIND == PASS_FORCE || KIND == PASS_SURFACE || KIND == PASS_ADJ_FORCE || KIND == PASS_ADJ_DENSITY;
+// Cubic spline divided by its factor 8/(pi h^3) (kernel.cuh:12-19), without
+// branches: 6q^3 - 6q^2 + 1 (q <= 1/2), 2(1-q)^3 (q <= 1), 0 beyond.
+__device__ __forceinline__ float cubic_shape(float q) {
+    const float t = 1.f - q;
+    const float inner = __fmaf_rn(6.f * q * q, q - 1.f, 1.f);
+    const float outer = 2.f * t * t * t;
+    return q <= 0.5f ? inner : (q <= 1.f ? outer : 0.f);
 }
 
-// Per-lane accumulators of every pass (unused members are eliminated).
-struct Acc {
-    float w;        // density: sum W (fluid), boundary: sum m_b W
-    float wb;
-    float4 a;       // pressure accel (fluid part) / surface force
-    float4 ab;      // boundary pressure accel (added after the fluid mass factor)
-    float4 nrm;     // normal
-    float4 vl;      // viscosity laplacian
-    u32 cnt;
-    // adjoint accumulators
-    float4 xb, vb;  // dL/dx_i, dL/dv_i contributions
-    float pt;       // sum_j -m (abar_i - abar_j) . F(r_ij)   (pressure coefficient sensitivity)
-    float bt;       // sum_b -m_b abar_i . F(r_ib)             (boundary pressure coefficient)
-    float vt;       // sum_j (v_ij . r_ij) G_ij (w_j . r_ij)   (viscosity rho_i sensitivity)
-};
+// |r| / h from r^2 with one reciprocal square root; 0 for coincident points.
+__device__ __forceinline__ float q_of(float r2, float& rinv, const DevParams& P) {
+    rinv = rsqrtf(fmaxf(r2, 1e-30f));
+    return r2 * rinv * P.inv_h;
+}
 
+// Fluid pair (i, candidate m of the staged chunk) contributions. v[] holds
+// the segment accumulators of the pass:
+//   DENSITY     v0 = sum W / cubic_factor
+//   FORCE       v0..2 = -sum (p_i/rho_i^2 + p_j/rho_j^2) g_s r, v3..5 = sum g_c r / rho_j,
+//               v6..8 = sum (v_ij . r) g_c r / (rho_j (r^2 + eps))
+//   SURFACE     v0..2 = sum (m r/|r| C(q) + n_i - n_j) / (rho_i + rho_j)
+//   ADJ_FORCE   v0..2 = dL/dx_i, v3..5 = dL/dv_i, v6 = pressure-coefficient term, v7 = viscosity rho term
+//   ADJ_DENSITY v0..2 = dL/dx_i
 template <int KIND>
-__device__ __forceinline__ void fluid_pair(Acc& acc, const HomeData& H, u32 j, float4 xj, float r2,
-                                           const DevParams& P, const TravArgs& a) {
-    const float q = sqrtf(r2) * P.inv_h;
-    if constexpr (KIND == PASS_DENSITY) {
-        acc.w += cubic_w(q, P);
-    } else if constexpr (KIND == PASS_FORCE) {
-        const float4 r = f4(H.x.x - xj.x, H.x.y - xj.y, H.x.z - xj.z);
-        const float dj = __ldg(a.rho + j);
-        const float pj = __ldg(a.prs + j);
-        const float4 vj = __ldg(a.vel + j);
-        const float sg = spiky_grad(q, P);
-        const float cg = cubic_grad(q, P);
-        const float dpj = pj / (dj * dj);
-        const float c = (H.dpi + dpj) * sg;
-        acc.a.x -= c * r.x; acc.a.y -= c * r.y; acc.a.z -= c * r.z;
-        const float cn = cg / dj;
-        acc.nrm.x += r.x * cn; acc.nrm.y += r.y * cn; acc.nrm.z += r.z * cn;
-        const float vr = (H.v.x - vj.x) * r.x + (H.v.y - vj.y) * r.y + (H.v.z - vj.z) * r.z;
-        const float s = vr * cg / (dj * (r2 + P.visc_eps));
-        acc.vl.x += s * r.x; acc.vl.y += s * r.y; acc.vl.z += s * r.z;
+__device__ __forceinline__ void fluid_pair(float* v, const HomeData& H, const WarpView<KIND>& S, u32 m,
+                                           float4 xj, float r2, const DevParams& P, const TravArgs& a) {
+    const float rx = H.x.x - xj.x, ry = H.x.y - xj.y, rz = H.x.z - xj.z;
+    if constexpr (KIND == PASS_FORCE) {
+        // spiky_grad / cubic_grad (kernel.cuh:22-51) as coefficients of r
+        const float4 sbj = S.sb[m];
+        float rinv;
+        const float q = q_of(r2, rinv, P);
+        const float t = 1.f - q;
+        const float kr = (q >= 1.e-9f && q <= 1.f) ? rinv * P.inv_h : 0.f;
+        const float sg = P.spiky_grad_factor * (t * t) * kr;
+        const float cg = P.cubic_grad_factor * (q <= 0.5f ? q * (3.f * q - 2.f) : -(t * t)) * kr;
+        const float c = (H.dpi + xj.w) * sg;
+        v[0] -= c * rx; v[1] -= c * ry; v[2] -= c * rz;
+        const float cn = cg * sbj.w;
+        v[3] += rx * cn; v[4] += ry * cn; v[5] += rz * cn;
+        const float vr = (H.v.x - sbj.x) * rx + (H.v.y - sbj.y) * ry + (H.v.z - sbj.z) * rz;
+        const float s = __fdividef(vr * cn, r2 + P.visc_eps);
+        v[6] += s * rx; v[7] += s * ry; v[8] += s * rz;
     } else if constexpr (KIND == PASS_SURFACE) {
-        if (r2 > 1e-6f) {
-            const float dj = __ldg(a.rho + j);
-            const float4 nj = __ldg(a.normal + j);
-            const float4 r = f4(H.x.x - xj.x, H.x.y - xj.y, H.x.z - xj.z);
-            const float len = sqrtf(r2);
-            const float c = cohesion(q, P);
-            const float inv = 1.f / (H.rho + dj);
-            acc.a.x += (P.mass * (r.x / len) * c + H.n.x - nj.x) * inv;
-            acc.a.y += (P.mass * (r.y / len) * c + H.n.y - nj.y) * inv;
-            acc.a.z += (P.mass * (r.z / len) * c + H.n.z - nj.z) * inv;
-        }
+        // cohesion (kernel.cuh:53-63); pairs closer than 1e-3 are skipped
+        const float4 nj = S.sb[m];
+        float rinv;
+        const float q = q_of(r2, rinv, P);
+        const float t = 1.f - q;
+        const float q3t3 = (q * q * q) * (t * t * t);
+        const float coh = P.cohesion_factor * (q <= 0.5f ? 2.f * q3t3 - 1.f / 64.f : (q <= 1.f ? q3t3 : 0.f));
+        const float inv = r2 > 1e-6f ? __fdividef(1.f, H.rho + xj.w) : 0.f;
+        const float cm = P.mass * coh * rinv;
+        v[0] += (cm * rx + H.n.x - nj.x) * inv;
+        v[1] += (cm * ry + H.n.y - nj.y) * inv;
+        v[2] += (cm * rz + H.n.z - nj.z) * inv;
     } else if constexpr (KIND == PASS_ADJ_FORCE) {
         // pressure: a_i = -m sum_j A_ij F(r_ij), F(r) = g_s(|r|) r, A_ij = p_i/rho_i^2 + p_j/rho_j^2
-        const float4 r = f4(H.x.x - xj.x, H.x.y - xj.y, H.x.z - xj.z);
+        const u32 j = S.cand[m];
         const float rl = sqrtf(r2);
+        const float q = rl * P.inv_h;
         const float dj = __ldg(a.rho + j);
         const float pj = __ldg(a.prs + j);
         const float4 aj = __ldg(a.adj_abar + j);
@@ -217,13 +320,13 @@ __device__ __forceinline__ void fluid_pair(Acc& acc, const HomeData& H, u32 j, f
         const float gsp = rl > 0.f ? spiky_grad_dr(q, rl, P) / rl : 0.f;
         const float A = H.dpi + pj / (dj * dj);
         const float dax = H.abar.x - aj.x, day = H.abar.y - aj.y, daz = H.abar.z - aj.z;
-        const float rda = r.x * dax + r.y * day + r.z * daz;
-        acc.pt += -P.mass * gs * rda;
+        const float rda = rx * dax + ry * day + rz * daz;
+        v[6] += -P.mass * gs * rda;
         // x_i: -m A J_F(r) (abar_i - abar_j), J_F = g_s I + (g_s'/|r|) r r^T
         const float cA = -P.mass * A;
-        acc.xb.x += cA * (gs * dax + gsp * rda * r.x);
-        acc.xb.y += cA * (gs * day + gsp * rda * r.y);
-        acc.xb.z += cA * (gs * daz + gsp * rda * r.z);
+        v[0] += cA * (gs * dax + gsp * rda * rx);
+        v[1] += cA * (gs * day + gsp * rda * ry);
+        v[2] += cA * (gs * daz + gsp * rda * rz);
         // viscosity: vlap_i = sum_j (u.r) G(|r|) r / rho_j, u = v_i - v_j, G = g_c / (r^2 + eps)
         const float4 vj = __ldg(a.vel + j);
         const float4 wj = __ldg(a.adj_w + j);
@@ -233,72 +336,280 @@ __device__ __forceinline__ void fluid_pair(Acc& acc, const HomeData& H, u32 j, f
         const float G = gc / den;
         const float Gp = rl > 0.f ? (gcp / den - 2.f * rl * gc / (den * den)) / rl : 0.f;  // G'/|r|
         const float ux = H.v.x - vj.x, uy = H.v.y - vj.y, uz = H.v.z - vj.z;
-        const float ur = ux * r.x + uy * r.y + uz * r.z;
-        const float wir = H.w.x * r.x + H.w.y * r.y + H.w.z * r.z;
-        const float wjr = wj.x * r.x + wj.y * r.y + wj.z * r.z;
+        const float ur = ux * rx + uy * ry + uz * rz;
+        const float wir = H.w.x * rx + H.w.y * ry + H.w.z * rz;
+        const float wjr = wj.x * rx + wj.y * ry + wj.z * rz;
         const float inv_dj = 1.f / dj, inv_di = 1.f / H.rho;
         const float cv = G * (wir * inv_dj - wjr * inv_di);
-        acc.vb.x += cv * r.x; acc.vb.y += cv * r.y; acc.vb.z += cv * r.z;
-        acc.vt += ur * G * wjr;
+        v[3] += cv * rx; v[4] += cv * ry; v[5] += cv * rz;
+        v[7] += ur * G * wjr;
         const float si = inv_dj, sj = inv_di;
-        acc.xb.x += si * (ux * G * wir + ur * G * H.w.x + ur * wir * Gp * r.x) -
-                    sj * (ux * G * wjr + ur * G * wj.x + ur * wjr * Gp * r.x);
-        acc.xb.y += si * (uy * G * wir + ur * G * H.w.y + ur * wir * Gp * r.y) -
-                    sj * (uy * G * wjr + ur * G * wj.y + ur * wjr * Gp * r.y);
-        acc.xb.z += si * (uz * G * wir + ur * G * H.w.z + ur * wir * Gp * r.z) -
-                    sj * (uz * G * wjr + ur * G * wj.z + ur * wjr * Gp * r.z);
+        v[0] += si * (ux * G * wir + ur * G * H.w.x + ur * wir * Gp * rx) -
+                sj * (ux * G * wjr + ur * G * wj.x + ur * wjr * Gp * rx);
+        v[1] += si * (uy * G * wir + ur * G * H.w.y + ur * wir * Gp * ry) -
+                sj * (uy * G * wjr + ur * G * wj.y + ur * wjr * Gp * ry);
+        v[2] += si * (uz * G * wir + ur * G * H.w.z + ur * wir * Gp * rz) -
+                sj * (uz * G * wjr + ur * G * wj.z + ur * wjr * Gp * rz);
     } else if constexpr (KIND == PASS_ADJ_DENSITY) {
         // rho_i = m (W(0) + sum_j W(|r_ij|)): dW/dx_i = g_c r_ij, shared by rho_i and rho_j
+        const u32 j = S.cand[m];
+        const float q = sqrtf(r2) * P.inv_h;
         const float rb = __ldg(a.adj_rhobar + j);
         const float c = P.mass * cubic_grad(q, P) * (H.rb + rb);
-        const float4 r = f4(H.x.x - xj.x, H.x.y - xj.y, H.x.z - xj.z);
-        acc.xb.x += c * r.x; acc.xb.y += c * r.y; acc.xb.z += c * r.z;
+        v[0] += c * rx; v[1] += c * ry; v[2] += c * rz;
     }
 }
 
+// Boundary pair contributions; v[] of the pass:
+//   DENSITY v0 = sum m_b W / cubic_factor; FORCE v0..2 = boundary pressure accel;
+//   ADJ_FORCE v0..2 = dL/dx_i, v3 = boundary pressure-coefficient term; ADJ_DENSITY v0..2 = dL/dx_i
 template <int KIND>
-__device__ __forceinline__ void boundary_pair(Acc& acc, const HomeData& H, u32 b, float4 xb, float r2,
+__device__ __forceinline__ void boundary_pair(float* v, const HomeData& H, u32 b, float4 xb, float r2,
                                               const DevParams& P, const TravArgs& a) {
-    const float q = sqrtf(r2) * P.inv_h;
     const float mb = __ldg(a.bmass + b);
+    const float rx = H.x.x - xb.x, ry = H.x.y - xb.y, rz = H.x.z - xb.z;
     if constexpr (KIND == PASS_DENSITY) {
-        acc.wb += cubic_w(q, P) * mb;
+        float rinv;
+        v[0] += cubic_shape(q_of(r2, rinv, P)) * mb;
     } else if constexpr (KIND == PASS_FORCE) {
-        const float b_p_term = H.dpi + H.prs / P.rest_density2;
-        const float c = mb * b_p_term * spiky_grad(q, P);
-        acc.ab.x -= c * (H.x.x - xb.x);
-        acc.ab.y -= c * (H.x.y - xb.y);
-        acc.ab.z -= c * (H.x.z - xb.z);
+        const float q = sqrtf(r2) * P.inv_h;
+        const float c = mb * (H.dpi + H.prs / P.rest_density2) * spiky_grad(q, P);
+        v[0] -= c * rx; v[1] -= c * ry; v[2] -= c * rz;
     } else if constexpr (KIND == PASS_ADJ_FORCE) {
         // a_i -= m_b B_i F(r_ib), B_i = p_i/rho_i^2 + p_i/rho0^2
-        const float4 r = f4(H.x.x - xb.x, H.x.y - xb.y, H.x.z - xb.z);
         const float rl = sqrtf(r2);
+        const float q = rl * P.inv_h;
         const float gs = spiky_grad(q, P);
         const float gsp = rl > 0.f ? spiky_grad_dr(q, rl, P) / rl : 0.f;
         const float B = H.dpi + H.prs / P.rest_density2;
-        const float ra = r.x * H.abar.x + r.y * H.abar.y + r.z * H.abar.z;
-        acc.bt += -mb * gs * ra;
+        const float ra = rx * H.abar.x + ry * H.abar.y + rz * H.abar.z;
+        v[3] += -mb * gs * ra;
         const float cB = -mb * B;
-        acc.xb.x += cB * (gs * H.abar.x + gsp * ra * r.x);
-        acc.xb.y += cB * (gs * H.abar.y + gsp * ra * r.y);
-        acc.xb.z += cB * (gs * H.abar.z + gsp * ra * r.z);
+        v[0] += cB * (gs * H.abar.x + gsp * ra * rx);
+        v[1] += cB * (gs * H.abar.y + gsp * ra * ry);
+        v[2] += cB * (gs * H.abar.z + gsp * ra * rz);
     } else if constexpr (KIND == PASS_ADJ_DENSITY) {
-        const float c = mb * H.rb * cubic_grad(q, P);
-        acc.xb.x += c * (H.x.x - xb.x);
-        acc.xb.y += c * (H.x.y - xb.y);
-        acc.xb.z += c * (H.x.z - xb.z);
+        const float c = mb * H.rb * cubic_grad(sqrtf(r2) * P.inv_h, P);
+        v[0] += c * rx; v[1] += c * ry; v[2] += c * rz;
     }
+}
+
+// ---------------------------------------------------------------------------
+// Segmented runs. A block of nh home particles (rows) is processed as one
+// flat item space split into 32 contiguous runs, one per lane, so every lane
+// does the same amount of work whatever the home count. A lane's run crosses
+// rows in order; it stores one partial per (lane, row) segment in slot
+// lane + row (unique: a later lane never reaches an earlier row), and
+// combine() then adds, on lane k, the partials of row k in lane order, so
+// the sums are deterministic.
+// ---------------------------------------------------------------------------
+template <int NF>
+__device__ __forceinline__ void store_partial(float* part, u32 slot, const float* v) {
+#pragma unroll
+    for (int f = 0; f < NF; ++f) part[slot * NF + f] = v[f];
+}
+
+// Row k = lane owns items [lo, hi); c = run length.
+template <int NF>
+__device__ __forceinline__ void combine(const float* part, float* res, bool active, u32 lo, u32 hi, u32 c) {
+    const u32 k = lane_id();
+    if (active && hi > lo) {
+        const u32 l_lo = lo / c, l_hi = (hi - 1) / c;
+        for (u32 l = l_lo; l <= l_hi; ++l) {
+#pragma unroll
+            for (int f = 0; f < NF; ++f) res[f] += part[(l + k) * NF + f];
+        }
+    }
+    __syncwarp();
+}
+
+// Fluid pairs rows [0, nh) x staged candidates [0, len) (candidate index
+// c0 + m), each tested against h^2 and the home particle itself (candidate
+// index self0 + row). BITS: the neighbour bits go to the block's bit matrix
+// in S.aux (row-major, row length len). Returns the run length.
+template <int KIND, bool BITS>
+__device__ __forceinline__ u32 fluid_pair_run(const WarpView<KIND>& S, const DevParams& P, const TravArgs& a,
+                                              u32 nh, u32 len, u32 c0, u32 i0, u32 self0) {
+    constexpr int NF = KindCfg<KIND>::nf;
+    const u32 lane = lane_id();
+    const u32 total = nh * len;
+    const u32 c = ((total + 31u) >> 5) | 1u;  // odd: spreads the lanes' staged reads over the banks
+    u32 p = lane * c;
+    const u32 e = min(p + c, total);
+    if (p < e) {
+        u32 k = p / len;
+        u32 m = p - k * len;
+        HomeData H = load_home<KIND>(a, i0 + k);
+        u32 self = self0 + k - c0;
+        float v[NF];
+#pragma unroll
+        for (int f = 0; f < NF; ++f) v[f] = 0.f;
+        u32 wbits = 0;
+        for (;;) {
+            const float4 xj = S.sa[m];
+            const float r2 = dist2(H.x, xj);
+            const bool nb = r2 <= P.h2 && m != self;
+            if constexpr (BITS) {
+                wbits |= static_cast<u32>(nb) << (p & 31u);
+                if ((p & 31u) == 31u || p + 1 == e) {
+                    if (wbits) atomicOr(S.aux + (p >> 5), wbits);
+                    wbits = 0;
+                }
+            }
+            if constexpr (KIND == PASS_DENSITY) {
+                float rinv;
+                const float w = cubic_shape(q_of(r2, rinv, P));
+                v[0] += nb ? w : 0.f;
+            } else {
+                if (nb) fluid_pair<KIND>(v, H, S, m, xj, r2, P, a);
+            }
+            ++p;
+            if (++m == len || p == e) {
+                store_partial<NF>(S.part, lane + k, v);
+                if (p == e) break;
+#pragma unroll
+                for (int f = 0; f < NF; ++f) v[f] = 0.f;
+                m = 0;
+                ++k;
+                H = load_home<KIND>(a, i0 + k);
+                self = self0 + k - c0;
+            }
+        }
+    }
+    __syncwarp();
+    return c;
+}
+
+// Neighbour pairs of rows [0, nh) read from the block's bit matrix in
+// global memory (bits, row length M), split by hits. Returns the run length
+// (0: no hits) and, for row k = lane, its hit range [lo, hi).
+template <int KIND>
+__device__ __forceinline__ u32 fluid_hit_run(const WarpView<KIND>& S, const DevParams& P, const TravArgs& a,
+                                             const u32* __restrict__ bits, u32 nh, u32 M, u32 i0, u32& lo,
+                                             u32& hi) {
+    constexpr int NF = KindCfg<KIND>::nf;
+    const u32 lane = lane_id();
+    const u32 nwords = (nh * M + 31u) >> 5;
+    u32 cnt = 0;
+    if (lane < nh) {
+        const u32 b0 = lane * M, b1 = b0 + M - 1;
+        const u32 w0 = b0 >> 5, w1 = b1 >> 5;
+        for (u32 w = w0; w <= w1; ++w) {
+            u32 x = __ldg(bits + w);
+            if (w == w0) x &= FULL << (b0 & 31u);
+            if (w == w1) x &= FULL >> (31u - (b1 & 31u));
+            cnt += __popc(x);
+        }
+    }
+    const u32 incl = warp_incl_scan(cnt);
+    const u32 total = __shfl_sync(FULL, incl, 31);
+    u32* hoff = S.aux;
+    lo = incl - cnt;
+    hi = incl;
+    if (lane < nh) hoff[lane] = lo;
+    if (lane == 0) hoff[nh] = total;
+    __syncwarp();
+    if (total == 0) return 0;
+    const u32 c = (total + 31u) >> 5;
+    u32 h = lane * c;
+    const u32 e = min(h + c, total);
+    if (h < e) {
+        u32 k = 0, kh = nh;  // the row holding hit h: largest k with hoff[k] <= h
+        while (kh - k > 1) {
+            const u32 mid = (k + kh) >> 1;
+            if (hoff[mid] <= h) k = mid; else kh = mid;
+        }
+        u32 r = h - hoff[k];
+        u32 row0 = k * M;
+        u32 wr = row0 >> 5;
+        u32 word = __ldg(bits + wr) & (FULL << (row0 & 31u));
+        for (;;) {
+            const u32 pc = __popc(word);
+            if (r < pc || wr + 1 >= nwords) break;
+            r -= pc;
+            word = __ldg(bits + ++wr);
+        }
+        for (; r && word; --r) word &= word - 1;
+        HomeData H = load_home<KIND>(a, i0 + k);
+        float v[NF];
+#pragma unroll
+        for (int f = 0; f < NF; ++f) v[f] = 0.f;
+        while (word) {
+            const u32 b = __ffs(word) - 1;
+            word &= word - 1;
+            const u32 p = (wr << 5) + b;
+            if (p >= row0 + M) {
+                store_partial<NF>(S.part, lane + k, v);
+#pragma unroll
+                for (int f = 0; f < NF; ++f) v[f] = 0.f;
+                do { ++k; row0 += M; } while (p >= row0 + M);
+                H = load_home<KIND>(a, i0 + k);
+            }
+            const u32 m = p - row0;
+            const float4 xj = S.sa[m];
+            fluid_pair<KIND>(v, H, S, m, xj, dist2(H.x, xj), P, a);
+            if (++h == e) break;
+            while (word == 0 && wr + 1 < nwords) word = __ldg(bits + ++wr);
+        }
+        store_partial<NF>(S.part, lane + k, v);
+    }
+    __syncwarp();
+    return c;
+}
+
+// Boundary pairs rows [0, nh) x expanded boundary candidates [0, len).
+template <int KIND>
+__device__ __forceinline__ u32 boundary_pair_run(const WarpView<KIND>& S, const DevParams& P, const TravArgs& a,
+                                                 u32 nh, u32 len, u32 i0) {
+    constexpr int NFB = KindCfg<KIND>::nfb;
+    const u32 lane = lane_id();
+    const u32 total = nh * len;
+    const u32 c = ((total + 31u) >> 5) | 1u;
+    u32 p = lane * c;
+    const u32 e = min(p + c, total);
+    if (p < e) {
+        u32 k = p / len;
+        u32 m = p - k * len;
+        HomeData H = load_home<KIND>(a, i0 + k);
+        float v[NFB];
+#pragma unroll
+        for (int f = 0; f < NFB; ++f) v[f] = 0.f;
+        for (;;) {
+            const u32 b = S.bcand[m];
+            const float4 xb = __ldg(a.bpos + b);
+            const float r2 = dist2(H.x, xb);
+            if (r2 <= P.h2) boundary_pair<KIND>(v, H, b, xb, r2, P, a);
+            ++p;
+            if (++m == len || p == e) {
+                store_partial<NFB>(S.part, lane + k, v);
+                if (p == e) break;
+#pragma unroll
+                for (int f = 0; f < NFB; ++f) v[f] = 0.f;
+                m = 0;
+                ++k;
+                H = load_home<KIND>(a, i0 + k);
+            }
+        }
+    }
+    __syncwarp();
+    return c;
 }
 
 template <int KIND, int WPB, bool BATCH>
 __global__ void __launch_bounds__(WPB * 32) cell_pass_kernel(const DevParams P, const TravArgs a) {
-    __shared__ WarpSmem smem[WPB];
+    using C = KindCfg<KIND>;
+    constexpr int NF = C::nf;
+    constexpr int NFB = C::nfb;
+    extern __shared__ __align__(16) unsigned char dyn_smem[];
     __shared__ float s_dt, s_np_dt;
     __shared__ float s_red[WPB][3];
     __shared__ bool s_last;
     const u32 lane = lane_id();
     const u32 warp = threadIdx.x >> 5;
-    WarpSmem& S = smem[warp];
+    const u32 cap = a.mask_words * 32u;
+    WarpView<KIND> S;
+    const size_t wbytes = warp_smem_bytes<KIND>(cap);
+    warp_smem_bytes<KIND>(cap, &S, dyn_smem + warp * wbytes);
 
     float dt = 0.f, np_dt = 0.f;
     if constexpr (KIND == PASS_SURFACE) {
@@ -319,14 +630,13 @@ __global__ void __launch_bounds__(WPB * 32) cell_pass_kernel(const DevParams P, 
     const u32 D = static_cast<u32>(2 * R + 1);
     const u32 ncell = D * D * D;
     const u32 qc = ncell >> 1;
-    const u32 cap = a.mask_words * 32u;
 
     if (base < n) {
-        const u32 i0 = base + lane;
-        const u64 my_pk = i0 < n ? a.ckey[i0] : 0ull;
+        const u32 i0l = base + lane;
+        const u64 my_pk = i0l < n ? a.ckey[i0l] : 0ull;
         u64 prev_pk = __shfl_up_sync(FULL, my_pk, 1);
-        if (lane == 0) prev_pk = i0 > 0 ? a.ckey[i0 - 1] : ~my_pk;
-        u32 starts = __ballot_sync(FULL, i0 < n && (i0 == 0 || my_pk != prev_pk));
+        if (lane == 0) prev_pk = i0l > 0 ? a.ckey[i0l - 1] : ~my_pk;
+        u32 starts = __ballot_sync(FULL, i0l < n && (i0l == 0 || my_pk != prev_pk));
         while (starts) {
             const u32 s = __ffs(starts) - 1;
             starts &= starts - 1;
@@ -352,14 +662,14 @@ __global__ void __launch_bounds__(WPB * 32) cell_pass_kernel(const DevParams P, 
             });
             const u32 home_start = S.rstart[qc];
             const u32 n_home = S.rpref[qc + 1] - S.rpref[qc];
+            const u32 self_base = S.rpref[qc];   // candidate index of the first home particle
             const bool masked = M <= cap;
-            const u32 nwords = (M + 31) >> 5;
 
             // boundary neighbour cells: union of the home particles' 3x3x3
             // boundary-cell neighbourhoods (cell size h, R = 1,
             // for_boundary_neighbors common.cuh:153-178)
             u32 MB = 0, nbc = 0;
-            if constexpr (uses_boundary<KIND>()) {
+            if constexpr (C::boundary) {
                 if (a.nb > 0) {
                     int lo[3] = {INT_MAX, INT_MAX, INT_MAX}, hi[3] = {INT_MIN, INT_MIN, INT_MIN};
                     for (u32 k = lane; k < n_home; k += 32) {
@@ -391,180 +701,132 @@ __global__ void __launch_bounds__(WPB * 32) cell_pass_kernel(const DevParams P, 
                 }
             }
 
-            if (masked && M > 0) expand(S.cand, S.rstart, S.rpref, ncell, 0, M);
+            if (masked) stage<KIND>(S, a, ncell, 0, M);
+            // the cell's neighbour bit matrix: row k = home particle k, bit m = candidate m
+            u32* const cell_bits = a.mask + static_cast<size_t>(home_start) * a.mask_words;
 
-            for (u32 hb = 0; hb < n_home; hb += 32) {
-                const u32 nh = min(32u, n_home - hb);
-                const u32 lg = nh <= 1 ? 0u : 32u - __clz(nh - 1);  // ceil(log2(nh))
-                const u32 L = 32u >> lg;
-                const u32 g = lane >> (5u - lg);
-                const u32 l = lane & (L - 1u);
-                const bool hv = g < nh;
-                const u32 i = home_start + hb + (hv ? g : 0u);
+            for (u32 hb = 0; hb < n_home; hb += HOME_BLOCK) {
+                const u32 nh = min(HOME_BLOCK, n_home - hb);
+                const u32 i0 = home_start + hb;
+                const u32 self0 = self_base + hb;
+                const bool act = lane < nh;
+                const u32 i = i0 + (act ? lane : 0u);
+                u32* const blk_bits = cell_bits + (hb >> 5) * M;   // row hb starts at bit hb * M
+                float res[NF], resb[NFB];
+#pragma unroll
+                for (int f = 0; f < NF; ++f) res[f] = 0.f;
+#pragma unroll
+                for (int f = 0; f < NFB; ++f) resb[f] = 0.f;
 
-                HomeData H;
-                H.x = a.pos[i];
-                if constexpr (KIND == PASS_FORCE || KIND == PASS_SURFACE) {
-                    H.v = a.vel[i];
-                    H.rho = a.rho[i];
-                    H.prs = a.prs[i];
-                    H.dpi = H.prs / (H.rho * H.rho);
-                }
-                if constexpr (KIND == PASS_SURFACE) {
-                    H.n = a.normal[i];
-                    H.ap = a.ap[i];
-                    H.vl = a.vlap[i];
-                }
-                if constexpr (KIND == PASS_ADJ_FORCE) {
-                    H.v = a.vel[i];
-                    H.rho = a.rho[i];
-                    H.prs = a.prs[i];
-                    H.dpi = H.prs / (H.rho * H.rho);
-                    H.abar = a.adj_abar[i];
-                    H.w = a.adj_w[i];
-                }
-                if constexpr (KIND == PASS_ADJ_DENSITY) H.rb = a.adj_rhobar[i];
-                Acc acc{};
-
-                if constexpr (KIND == PASS_DENSITY) {
-                    // full candidate scan; writes the neighbour bitmasks
-                    for (u32 c0 = 0; c0 < M; c0 += CAND_CAP) {
-                        const u32 len = min(static_cast<u32>(CAND_CAP), M - c0);
-                        if (!masked) expand(S.cand, S.rstart, S.rpref, ncell, c0, len);
-                        const u32 iters = (len + L - 1) / L;
-                        u32 word = 0;
-                        for (u32 it = 0; it < iters; ++it) {
-                            const u32 ml = it * L + l;
-                            bool nb = false;
-                            if (ml < len && hv) {
-                                const u32 j = S.cand[ml];
-                                const float4 xj = a.pos[j];
-                                const float r2 = dist2(H.x, xj);
-                                nb = (j != i) && (r2 <= P.h2);
-                                if (nb) fluid_pair<KIND>(acc, H, j, xj, r2, P, a);
-                            }
-                            if (masked) {
-                                const u32 bal = __ballot_sync(FULL, nb);
-                                const u32 gbits = L == 32u ? bal : ((bal >> (g * L)) & ((1u << L) - 1u));
-                                const u32 bitpos = (it * L) & 31u;
-                                word |= gbits << bitpos;
-                                if (bitpos + L == 32u || it + 1 == iters) {
-                                    if (l == 0 && hv) a.mask[static_cast<size_t>(i) * a.mask_words + ((c0 + it * L) >> 5)] = word;
-                                    word = 0;
-                                }
-                            }
-                        }
-                    }
-                } else if constexpr (uses_masks<KIND>()) {
+                if constexpr (KIND == PASS_COUNT || KIND == PASS_FILL) {
+                    // sequential per home particle, in candidate order (the reference's order)
+                    u32 cnt = 0;
+                    u32 wpos = 0;
+                    if constexpr (KIND == PASS_FILL) wpos = act ? a.offsets[i] : 0u;
                     if (masked) {
-                        if (hv) {
-                            const u32* mrow = a.mask + static_cast<size_t>(i) * a.mask_words;
-                            for (u32 w = l; w < nwords; w += L) {
-                                u32 bits = mrow[w];
-                                while (bits) {
-                                    const u32 b = __ffs(bits) - 1;
-                                    bits &= bits - 1;
-                                    const u32 j = S.cand[w * 32 + b];
-                                    const float4 xj = a.pos[j];
-                                    fluid_pair<KIND>(acc, H, j, xj, dist2(H.x, xj), P, a);
+                        if (act) {
+                            const u32 b0 = lane * M, b1 = b0 + M - 1;
+                            for (u32 w = b0 >> 5; w <= (b1 >> 5); ++w) {
+                                u32 x = blk_bits[w];
+                                if (w == (b0 >> 5)) x &= FULL << (b0 & 31u);
+                                if (w == (b1 >> 5)) x &= FULL >> (31u - (b1 & 31u));
+                                while (x) {
+                                    const u32 bit = __ffs(x) - 1;
+                                    x &= x - 1;
+                                    if constexpr (KIND == PASS_FILL) {
+                                        const u32 m = (w << 5) + bit - b0;
+                                        if (wpos < a.nbr_capacity) a.nbr_out[wpos] = S.cand[m];
+                                        ++wpos;
+                                    }
+                                    ++cnt;
                                 }
                             }
                         }
                     } else {
-                        for (u32 c0 = 0; c0 < M; c0 += CAND_CAP) {
-                            const u32 len = min(static_cast<u32>(CAND_CAP), M - c0);
-                            expand(S.cand, S.rstart, S.rpref, ncell, c0, len);
-                            if (hv) {
-                                for (u32 ml = l; ml < len; ml += L) {
-                                    const u32 j = S.cand[ml];
-                                    const float4 xj = a.pos[j];
-                                    const float r2 = dist2(H.x, xj);
-                                    if (j != i && r2 <= P.h2) fluid_pair<KIND>(acc, H, j, xj, r2, P, a);
+                        const float4 xi = a.pos[i];
+                        for (u32 c0 = 0; c0 < M; c0 += cap) {
+                            const u32 len = min(cap, M - c0);
+                            stage<KIND>(S, a, ncell, c0, len);
+                            if (act) {
+                                for (u32 ml = 0; ml < len; ++ml) {
+                                    if (c0 + ml != self0 + lane && dist2(xi, S.sa[ml]) <= P.h2) {
+                                        if constexpr (KIND == PASS_FILL) {
+                                            if (wpos < a.nbr_capacity) a.nbr_out[wpos] = S.cand[ml];
+                                            ++wpos;
+                                        }
+                                        ++cnt;
+                                    }
                                 }
                             }
                         }
                     }
-                } else {  // PASS_COUNT / PASS_FILL: sequential in candidate order (reference order)
-                    u32 wpos = 0;
-                    if constexpr (KIND == PASS_FILL) wpos = hv ? a.offsets[i] : 0u;
-                    for (u32 c0 = 0; c0 < M; c0 += CAND_CAP) {
-                        const u32 len = min(static_cast<u32>(CAND_CAP), M - c0);
-                        if (!masked) expand(S.cand, S.rstart, S.rpref, ncell, c0, len);
-                        if (hv && l == 0) {
-                            for (u32 ml = 0; ml < len; ++ml) {
-                                const u32 j = S.cand[ml];
-                                bool nb;
-                                if (masked) {
-                                    nb = (a.mask[static_cast<size_t>(i) * a.mask_words + (ml >> 5)] >> (ml & 31)) & 1u;
-                                } else {
-                                    nb = (j != i) && dist2(H.x, a.pos[j]) <= P.h2;
-                                }
-                                if (nb) {
-                                    if constexpr (KIND == PASS_FILL) {
-                                        if (wpos < a.nbr_capacity) a.nbr_out[wpos] = j;
-                                        ++wpos;
-                                    }
-                                    ++acc.cnt;
-                                }
-                            }
+                    if constexpr (KIND == PASS_COUNT) {
+                        if (act) a.counts[i] = cnt;
+                    }
+                    continue;
+                } else if constexpr (KIND == PASS_DENSITY) {
+                    if (masked) {
+                        const u32 nwords = (nh * M + 31u) >> 5;
+                        for (u32 w = lane; w < nwords; w += 32) S.aux[w] = 0u;
+                        __syncwarp();
+                        const u32 c = fluid_pair_run<KIND, true>(S, P, a, nh, M, 0, i0, self0);
+                        combine<NF>(S.part, res, act, lane * M, lane * M + M, c);
+                        for (u32 w = lane; w < nwords; w += 32) blk_bits[w] = S.aux[w];
+                        __syncwarp();
+                    } else {
+                        for (u32 c0 = 0; c0 < M; c0 += cap) {
+                            const u32 len = min(cap, M - c0);
+                            stage<KIND>(S, a, ncell, c0, len);
+                            const u32 c = fluid_pair_run<KIND, false>(S, P, a, nh, len, c0, i0, self0);
+                            combine<NF>(S.part, res, act, lane * len, lane * len + len, c);
+                        }
+                    }
+                } else {
+                    if (masked) {
+                        u32 lo, hi;
+                        const u32 c = fluid_hit_run<KIND>(S, P, a, blk_bits, nh, M, i0, lo, hi);
+                        if (c) combine<NF>(S.part, res, act, lo, hi, c);
+                    } else {
+                        for (u32 c0 = 0; c0 < M; c0 += cap) {
+                            const u32 len = min(cap, M - c0);
+                            stage<KIND>(S, a, ncell, c0, len);
+                            const u32 c = fluid_pair_run<KIND, false>(S, P, a, nh, len, c0, i0, self0);
+                            combine<NF>(S.part, res, act, lane * len, lane * len + len, c);
                         }
                     }
                 }
 
                 // boundary candidates (density and pressure passes)
-                if constexpr (uses_boundary<KIND>()) {
+                if constexpr (C::boundary) {
                     for (u32 c0 = 0; c0 < MB; c0 += BCAND_CAP) {
-                        const u32 len = min(static_cast<u32>(BCAND_CAP), MB - c0);
+                        const u32 len = min(BCAND_CAP, MB - c0);
                         expand(S.bcand, S.bstart, S.bpref, nbc, c0, len);
-                        if (hv) {
-                            for (u32 ml = l; ml < len; ml += L) {
-                                const u32 b = S.bcand[ml];
-                                const float4 xb = a.bpos[b];
-                                const float r2 = dist2(H.x, xb);
-                                if (r2 <= P.h2) boundary_pair<KIND>(acc, H, b, xb, r2, P, a);
-                            }
-                        }
+                        const u32 c = boundary_pair_run<KIND>(S, P, a, nh, len, i0);
+                        combine<NFB>(S.part, resb, act, lane * len, lane * len + len, c);
                     }
                 }
 
-                // combine the L lanes of each group
-                if constexpr (KIND == PASS_DENSITY) {
-                    acc.w = group_sum<float>(acc.w, L);
-                    acc.wb = group_sum<float>(acc.wb, L);
-                } else if constexpr (KIND == PASS_FORCE) {
-                    acc.a = group_sum4(acc.a, L);
-                    acc.ab = group_sum4(acc.ab, L);
-                    acc.nrm = group_sum4(acc.nrm, L);
-                    acc.vl = group_sum4(acc.vl, L);
-                } else if constexpr (KIND == PASS_SURFACE) {
-                    acc.a = group_sum4(acc.a, L);
-                } else if constexpr (KIND == PASS_ADJ_FORCE) {
-                    acc.xb = group_sum4(acc.xb, L);
-                    acc.vb = group_sum4(acc.vb, L);
-                    acc.pt = group_sum<float>(acc.pt, L);
-                    acc.bt = group_sum<float>(acc.bt, L);
-                    acc.vt = group_sum<float>(acc.vt, L);
-                } else if constexpr (KIND == PASS_ADJ_DENSITY) {
-                    acc.xb = group_sum4(acc.xb, L);
-                }
-
-                if (hv && l == 0) {
+                if (act) {
                     if constexpr (KIND == PASS_DENSITY) {
                         // compute_density: (W(0) + sum W) * m, then + sum m_b W
-                        const float rho = (P.w0 + acc.w) * P.mass + acc.wb;
+                        const float rho = (P.w0 + P.cubic_factor * res[0]) * P.mass + P.cubic_factor * resb[0];
                         a.rho[i] = rho;
                         a.prs[i] = tait_pressure(rho, P);
                     } else if constexpr (KIND == PASS_FORCE) {
                         // compute_pressure_accel_n_normal_with_boundary: m * sum_fluid, then
                         // the boundary term (compute_pressure_accel_n_normal.cu:346-364)
-                        a.ap[i] = f4(P.mass * acc.a.x + acc.ab.x, P.mass * acc.a.y + acc.ab.y,
-                                     P.mass * acc.a.z + acc.ab.z);
+                        a.ap[i] = f4(P.mass * res[0] + resb[0], P.mass * res[1] + resb[1],
+                                     P.mass * res[2] + resb[2]);
                         const float sn = P.h * P.mass;
-                        a.normal[i] = f4(sn * acc.nrm.x, sn * acc.nrm.y, sn * acc.nrm.z);
-                        a.vlap[i] = acc.vl;
+                        a.normal[i] = f4(sn * res[3], sn * res[4], sn * res[5]);
+                        a.vlap[i] = f4(res[6], res[7], res[8]);
                     } else if constexpr (KIND == PASS_SURFACE) {
                         // a_np = g + F_ext + nu*10*m*vlap - alpha*2*rho0*f
-                        const float4 fe = external_force(H.x, P);
+                        const float4 xi = a.pos[i];
+                        const float4 vi = a.vel[i];
+                        const float4 api = a.ap[i];
+                        const float4 vli = a.vlap[i];
+                        const float4 fe = external_force(xi, P);
                         float4 gv = make_float4(P.gravity[0], P.gravity[1], P.gravity[2], P.visc_scale);
                         const DevBox* bb = a.box;
                         if constexpr (BATCH) {
@@ -573,16 +835,16 @@ __global__ void __launch_bounds__(WPB * 32) cell_pass_kernel(const DevParams P, 
                             a.scene_state[i] = scene;
                         }
                         float4 anp;
-                        anp.x = gv.x + fe.x + gv.w * H.vl.x - P.st_scale * acc.a.x;
-                        anp.y = gv.y + fe.y + gv.w * H.vl.y - P.st_scale * acc.a.y;
-                        anp.z = gv.z + fe.z + gv.w * H.vl.z - P.st_scale * acc.a.z;
+                        anp.x = gv.x + fe.x + gv.w * vli.x - P.st_scale * res[0];
+                        anp.y = gv.y + fe.y + gv.w * vli.y - P.st_scale * res[1];
+                        anp.z = gv.z + fe.z + gv.w * vli.z - P.st_scale * res[2];
                         anp.w = 0.f;
                         a.anp[i] = anp;
                         // update_positions.cu:64-67
-                        float4 v = H.v, x = H.x;
-                        v.x += np_dt * anp.x + dt * H.ap.x;
-                        v.y += np_dt * anp.y + dt * H.ap.y;
-                        v.z += np_dt * anp.z + dt * H.ap.z;
+                        float4 v = vi, x = xi;
+                        v.x += np_dt * anp.x + dt * api.x;
+                        v.y += np_dt * anp.y + dt * api.y;
+                        v.z += np_dt * anp.z + dt * api.z;
                         x.x += dt * v.x;
                         x.y += dt * v.y;
                         x.z += dt * v.z;
@@ -594,25 +856,28 @@ __global__ void __launch_bounds__(WPB * 32) cell_pass_kernel(const DevParams P, 
                         red_max = fmaxf(red_max, s2);
                         red_speed += sqrtf(s2);
                         red_speed2 += s2;
-                    } else if constexpr (KIND == PASS_COUNT) {
-                        a.counts[i] = acc.cnt;
                     } else if constexpr (KIND == PASS_ADJ_FORCE) {
-                        const float inv_r2 = 1.f / (H.rho * H.rho);
-                        const float pbar = acc.pt * inv_r2 + acc.bt * (inv_r2 + 1.f / P.rest_density2);
-                        float rhobar = (acc.pt + acc.bt) * (-2.f * H.prs * inv_r2 / H.rho) - acc.vt * inv_r2;
+                        const float rho_i = a.rho[i];
+                        const float prs_i = a.prs[i];
+                        const float pt = res[6], vt = res[7], bt = resb[3];
+                        const float inv_r2 = 1.f / (rho_i * rho_i);
+                        const float pbar = pt * inv_r2 + bt * (inv_r2 + 1.f / P.rest_density2);
+                        float rhobar = (pt + bt) * (-2.f * prs_i * inv_r2 / rho_i) + vt * inv_r2;
                         // Tait EOS with the clamp of compute_rho_p.cu:236-238
-                        const float ratio = H.rho / P.rest_density;
+                        const float ratio = rho_i / P.rest_density;
                         const float rc = fminf(fmaxf(ratio, 1.f), P.max_density_ratio);
                         if (ratio > 1.f && ratio < P.max_density_ratio)
                             rhobar += pbar * P.stiffness * P.exponent * powf(ratio, P.exponent - 1.f) / P.rest_density;
                         red_speed += pbar * (powf(rc, P.exponent) - 1.f);  // dL/dk partial
                         a.adj_rhobar[i] = rhobar;
-                        float4 xb0 = a.adj_xbar[i], vb0 = a.adj_vbar[i];
-                        a.adj_xbar[i] = f4(xb0.x + acc.xb.x, xb0.y + acc.xb.y, xb0.z + acc.xb.z);
-                        a.adj_vbar[i] = f4(vb0.x + acc.vb.x, vb0.y + acc.vb.y, vb0.z + acc.vb.z);
+                        const float4 xb0 = a.adj_xbar[i], vb0 = a.adj_vbar[i];
+                        a.adj_xbar[i] = f4(xb0.x + res[0] + resb[0], xb0.y + res[1] + resb[1],
+                                           xb0.z + res[2] + resb[2]);
+                        a.adj_vbar[i] = f4(vb0.x + res[3], vb0.y + res[4], vb0.z + res[5]);
                     } else if constexpr (KIND == PASS_ADJ_DENSITY) {
-                        float4 xb0 = a.adj_xbar[i];
-                        a.adj_xbar[i] = f4(xb0.x + acc.xb.x, xb0.y + acc.xb.y, xb0.z + acc.xb.z);
+                        const float4 xb0 = a.adj_xbar[i];
+                        a.adj_xbar[i] = f4(xb0.x + res[0] + resb[0], xb0.y + res[1] + resb[1],
+                                           xb0.z + res[2] + resb[2]);
                     }
                 }
             }
@@ -816,14 +1081,27 @@ void launch_reorder_cells(const float4* pos_in, const float4* vel_in, const u32*
                                                                   cend, tmask, st_err, nullptr);
 }
 
+template <int KIND, int WPB, bool BATCH>
+static void launch_wpb(const DevParams& P, const TravArgs& a, cudaStream_t stream, u32 grid) {
+    // per-warp candidate staging sized by the bit-matrix capacity 32 * mask_words
+    const size_t bytes = warp_smem_bytes<KIND>(a.mask_words * 32u) * WPB;
+    static bool configured = false;  // per instantiation; the attribute is per device function
+    if (!configured) {
+        cudaFuncSetAttribute(cell_pass_kernel<KIND, WPB, BATCH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(warp_smem_bytes<KIND>(32u * MAX_MASK_WORDS) * WPB));
+        configured = true;
+    }
+    cell_pass_kernel<KIND, WPB, BATCH><<<grid, WPB * 32, bytes, stream>>>(P, a);
+}
+
 template <int KIND, bool BATCH>
 static void launch_kind(const DevParams& P, const TravArgs& a, cudaStream_t stream, int wpb) {
     const u32 grid = pass_grid(a.n, wpb);
     if (grid == 0) return;
     switch (wpb) {
-    case 2: cell_pass_kernel<KIND, 2, BATCH><<<grid, 64, 0, stream>>>(P, a); break;
-    case 8: cell_pass_kernel<KIND, 8, BATCH><<<grid, 256, 0, stream>>>(P, a); break;
-    default: cell_pass_kernel<KIND, 4, BATCH><<<grid, 128, 0, stream>>>(P, a); break;
+    case 2: launch_wpb<KIND, 2, BATCH>(P, a, stream, grid); break;
+    case 8: launch_wpb<KIND, 8, BATCH>(P, a, stream, grid); break;
+    default: launch_wpb<KIND, 4, BATCH>(P, a, stream, grid); break;
     }
 }
 

@@ -14,13 +14,20 @@
 //                   CFL max |v|^2 and metric reductions
 //                   (compute_non_pressure_accel.cu + update_positions.cu:14-68)
 //
-// Work decomposition (all three passes): one warp per 32-particle chunk of
-// the sorted array; for every cell that starts inside the chunk, the warp
-// looks up the (2R+1)^3 neighbour cells once (lane-parallel hash probes),
-// expands their contiguous particle ranges into a shared-memory candidate
-// list, and assigns L = 32/next_pow2(n_home) lanes to each home particle.
-// Lanes stride the candidate list; partial sums are combined with xor
-// shuffles inside each L-lane group.
+// Work decomposition (all passes): one warp per 32-particle chunk of the
+// sorted array; for every cell that starts inside the chunk, the warp looks
+// up the (2R+1)^3 neighbour cells once (lane-parallel hash probes) and
+// stages their particles (the candidates, in the reference's cell order)
+// into shared memory. The home particles are taken in blocks of up to 32.
+// A block's work is a flat item space split into 32 contiguous lane runs,
+// so every lane does the same amount of work whatever the home count:
+//   density pass   items = (home, candidate) pairs; the distance test
+//                  writes the cell's neighbour bit matrix (row = home
+//                  particle, bit = candidate, row-major in the cell's
+//                  mask_words * n_home words of the mask buffer);
+//   later passes   items = the set bits of that matrix (neighbours only).
+// Each lane keeps one partial sum per home row it crosses; the partials are
+// added per home in lane order, so results are deterministic.
 #pragma once
 #include "sph_common.cuh"
 
@@ -29,6 +36,7 @@ namespace wcsph {
 constexpr int TRAV_WARPS = 4;            // warps per block of the traversal passes
 constexpr int MAX_RANGE_CELLS = 125;     // (2R+1)^3 with R <= 2
 constexpr int MAX_BOUNDARY_CELLS = 125;
+constexpr u32 MAX_MASK_WORDS = 16;      // bit-matrix words per particle (candidate cap = 32 * words)
 
 struct HashView {
     const u64* table;

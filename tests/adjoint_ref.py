@@ -14,6 +14,7 @@ from __future__ import annotations
 
 import numpy as np
 import torch
+from scipy.spatial import cKDTree
 from torch.utils.checkpoint import checkpoint
 
 
@@ -42,6 +43,7 @@ class Scene:
         self.v0 = torch.tensor(vel[:, :3], dtype=torch.float64)
         self.bpos = None if bpos is None else torch.tensor(bpos[:, :3], dtype=torch.float64)
         self.bmass = None if bmass is None else torch.tensor(bmass, dtype=torch.float64)
+        self._btree = None
 
     # ---- kernels as functions of q and |r| -------------------------------
     def W(self, q):
@@ -66,17 +68,28 @@ class Scene:
         # pairs at |r| ~ h contribute ~0 (every kernel vanishes there), so the
         # selection is made in float64 without the CUDA path's exact rounding
         xn = x.detach().numpy()
-        d = xn[:, None, :] - xn[None, :, :]
-        r2 = (d * d).sum(-1)
         h2 = float(np.float32(np.float32(self.h) * np.float32(self.h)))
-        m = r2 <= h2
-        np.fill_diagonal(m, False)
-        i, j = np.nonzero(m)
+        reach = np.sqrt(h2) * (1.0 + 1e-9)
+        tree = cKDTree(xn)
+        pr = tree.query_pairs(reach, output_type="ndarray")
+        if len(pr):
+            d = xn[pr[:, 0]] - xn[pr[:, 1]]
+            pr = pr[(d * d).sum(1) <= h2]
+        i = np.concatenate([pr[:, 0], pr[:, 1]]).astype(np.int64)
+        j = np.concatenate([pr[:, 1], pr[:, 0]]).astype(np.int64)
+        order = np.lexsort((j, i))
+        i, j = i[order], j[order]
         bi = bj = None
         if self.bpos is not None:
-            bn = self.bpos.numpy()
-            db = xn[:, None, :] - bn[None, :, :]
-            bi, bj = np.nonzero((db * db).sum(-1) <= h2)
+            if self._btree is None:
+                self._btree = cKDTree(self.bpos.numpy())
+            hits = tree.query_ball_tree(self._btree, reach)
+            bi = np.repeat(np.arange(len(hits)), [len(h) for h in hits]).astype(np.int64)
+            bj = np.fromiter((b for h in hits for b in sorted(h)), np.int64, count=len(bi))
+            if len(bi):
+                db = xn[bi] - self.bpos.numpy()[bj]
+                keep = (db * db).sum(1) <= h2
+                bi, bj = bi[keep], bj[keep]
         return i, j, bi, bj
 
     def step(self, x, v, nu, k, dt):
@@ -137,7 +150,7 @@ def reference_gradients(scene: Scene, nu: float, k: float, steps: int, dt: float
     tgt = torch.tensor(target[:, :3], dtype=torch.float64)
     loss = scene.rollout(v0, nu_t, k_t, steps, dt, tgt)
     loss.backward()
-    return float(loss), v0.grad.numpy(), float(nu_t.grad), float(k_t.grad)
+    return float(loss.detach()), v0.grad.numpy(), float(nu_t.grad), float(k_t.grad)
 
 
 def fd_gradient(scene: Scene, nu: float, k: float, steps: int, dt: float, target: np.ndarray, which: str,

@@ -1,0 +1,153 @@
+"""Headless CLI end to end, the autotuner, and long-run CSV statistics
+against the reference's own kernels (GPU)."""
+import csv
+import json
+import subprocess
+import sys
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import oracle
+import refpath
+import wcsph
+from parity import check_fields, dam_break_scene, oracle_one_step, pressure_bounds
+
+pytestmark = pytest.mark.gpu
+ROOT = Path(__file__).resolve().parent.parent
+CLI = ROOT / "fluid-simulation_b200" / "bin" / "wcsph_headless"
+
+
+def run_cli(*args, timeout=300):
+    return subprocess.run([str(CLI), *args], capture_output=True, text=True, timeout=timeout)
+
+
+def test_cli_snapshot_round_trip_and_csv(tmp_path):
+    snap = tmp_path / "s.sphs"
+    log = tmp_path / "log.csv"
+    r = run_cli("--scene", "tilting_box", "--headless", "--stop", "iters=6", "--fixed-dt", "0.01",
+                "--tuning-budget", "0", "--log-csv", str(log), "--log-metrics", "--snapshot-save", str(snap))
+    assert r.returncode == 0, r.stderr
+    rows = list(csv.reader(log.open()))
+    assert rows[0] == ["step", "sim_time", "wall_dt_ms", "scheduled_tune", "mean_speed", "ke"]
+    assert len(rows) == 7 and [int(x[0]) for x in rows[1:]] == list(range(6))
+    assert abs(float(rows[-1][1]) - 0.06) < 1e-9
+    assert wcsph.snapshot_header(snap) == ("tilting_box", 27000)
+    pos, vel = wcsph.snapshot_read(snap, "tilting_box", 27000)
+    # the metrics column matches the saved state
+    sp = np.linalg.norm(vel[:, :3].astype(np.float64), axis=1)
+    assert abs(float(rows[-1][4]) - sp.mean()) <= 1e-4 * sp.mean()
+    r = run_cli("--scene", "tilting_box", "--headless", "--stop", "sim-time=0.02", "--snapshot-load", str(snap),
+                "--tuning-budget", "0")
+    assert r.returncode == 0, r.stderr
+    r = run_cli("--scene", "surface_tension", "--headless", "--stop", "iters=1", "--snapshot-load", str(snap))
+    assert r.returncode == 1
+    assert "Snapshot load failed: Snapshot::load: app_name mismatch (file='tilting_box', expected='surface_tension')" \
+        in r.stderr
+
+
+def test_cli_tuning_writes_ktt_results(tmp_path):
+    out = tmp_path / "res.json"
+    r = run_cli("--scene", "surface_tension", "--headless", "--stop", "iters=8", "--tuning-budget", "1",
+                "--searcher", "random", "--ktt-output", str(out), "--warmup-iters", "2")
+    assert r.returncode == 0, r.stderr
+    res = json.loads(out.read_text())["Results"]
+    assert len(res) == 8
+    for e in res:
+        assert e["TotalDuration"] > 0 and e["ComputationResults"][0]["Duration"] > 0
+        names = {c["Name"] for c in e["Configuration"]}
+        assert {"CELL_SIZE_MULT", "TABLE_SIZE_MULT", "compute_rho_p_block"} <= names
+
+
+def test_tuner_searchers_and_frozen_config(tmp_path):
+    p, bx, pos, bpos = dam_break_scene(dims=(12, 12, 12))
+    for searcher in (wcsph.SEARCH_MCMC, wcsph.SEARCH_RANDOM, wcsph.SEARCH_FULL):
+        sim = wcsph.CUDASPHSimulator(p, pos, bx, boundary_pos=bpos)
+        sim.set_tuning(searcher, 1.0)
+        for _ in range(5):
+            sim.update(1e-3)
+            assert sim.was_scheduled_step()
+        sim.set_tuning(searcher, 0.0)
+        sim.update(1e-3)
+        assert not sim.was_scheduled_step()
+        cfg = tmp_path / f"best_{searcher}.json"
+        sim.save_config(cfg)
+        entries = json.loads(cfg.read_text())
+        assert {e["Name"] for e in entries} >= {"CELL_SIZE_MULT", "TABLE_SIZE_MULT"}
+        sim.close()
+    # a frozen config in the reference's schema (measurements/configs/*.json)
+    frozen = tmp_path / "frozen.json"
+    frozen.write_text(json.dumps([
+        {"Name": "CELL_SIZE_MULT", "Value": 0.6666666666666666, "ValueType": "Double"},
+        {"Name": "TABLE_SIZE_MULT", "Value": 16, "ValueType": "UnsignedInt"},
+        {"Name": "compute_rho_p_block", "Value": 64, "ValueType": "UnsignedInt"},
+        {"Name": "KERNEL_DIR", "Value": "/somewhere", "ValueType": "String"},
+        {"Name": "compute_rho_p_u_n", "Value": 4, "ValueType": "UnsignedInt"},
+    ]))
+    sim = wcsph.CUDASPHSimulator(p, pos, bx, boundary_pos=bpos)
+    sim.set_tuning(wcsph.SEARCH_MCMC, 0.1, frozen)
+    sim.update(1e-3)
+    assert not sim.was_scheduled_step()
+    got = {k: sim.field(k) for k in ("density", "pressure", "pressure_accel", "non_pressure_accel", "normal",
+                                     "position", "velocity", "morton_keys", "permutation")}
+    sim.close()
+    p2 = wcsph.Params.from_buffer_copy(p)
+    p2.cell_size_mult = float(np.float32(0.6666666666666666))
+    p2.table_size_mult = 16
+    ref, bs, bm = oracle_one_step(p2, bx, pos, np.zeros_like(pos), bpos, 1e-3)
+    assert np.array_equal(got["morton_keys"], ref.keys) and np.array_equal(got["permutation"], ref.perm)
+    want = {"density": ref.rho, "pressure": ref.prs, "pressure_accel": ref.ap, "non_pressure_accel": ref.anp,
+            "normal": ref.normal, "position": ref.pos, "velocity": ref.vel}
+    b = pressure_bounds(p2, ref.rho, ref.prs, pos[ref.perm], (ref.nbr_counts, ref.nbr_offsets, ref.nbr_idx), bs, bm,
+                        dt=ref.dt_p)
+    assert not check_fields(got, want, b)
+    bad = tmp_path / "bad.json"
+    bad.write_text('[{"Name": "CELL_SIZE_MULT", "Value": 0.5}]')
+    sim = wcsph.CUDASPHSimulator(p, pos, bx, boundary_pos=bpos)
+    with pytest.raises(wcsph.WcsphError) as e:
+        sim.set_tuning(wcsph.SEARCH_MCMC, 0.1, bad)
+    assert e.value.status == wcsph.ERR_CONFIG and "missing Name, Value, or ValueType" in e.value.message
+    sim.close()
+
+
+REF_STATS = r"""
+import sys, json, numpy as np
+sys.path[:0] = [sys.argv[1] + '/oracle', sys.argv[1] + '/fluid-simulation_b200']
+import refpath, wcsph
+pre = wcsph.preset('dam_break')
+sim = refpath.RefSim('dam_break', pre.pos, pre.vel, pre.bpos, pre.box)
+mass = 1000.0 * float(np.float32(np.float64(np.float32(0.02) ** 3) * 0.8))
+ms, ke = [], []
+for s in range(int(sys.argv[2])):
+    sim.step(pre.info.delta)
+    v = sim.fields()['velocity'][:, :3].astype(np.float64)
+    sp = np.linalg.norm(v, axis=1)
+    ms.append(sp.mean()); ke.append(0.5 * mass * (sp ** 2).sum())
+sim.close()
+print(json.dumps({'mean_speed': ms, 'ke': ke}))
+"""
+
+
+def test_long_run_statistics_match_reference_kernels():
+    """mean_speed / ke time averages of a 300-step dam break (32,768 particles
+    + walls) within 1% of the reference's own CUDA path on the same input."""
+    if not refpath.available("dam_break"):
+        pytest.skip("reference harness for dam_break not built")
+    steps = 300
+    out = subprocess.run([sys.executable, "-c", REF_STATS, str(ROOT), str(steps)], capture_output=True, text=True,
+                         timeout=900, check=True)
+    ref = json.loads(out.stdout.strip().splitlines()[-1])
+    pre = wcsph.preset("dam_break")
+    sim = pre.simulator()
+    ms, ke = [], []
+    for _ in range(steps):
+        sim.update(pre.info.delta)
+        a, b = sim.compute_state_metrics()
+        ms.append(a)
+        ke.append(b)
+    sim.close()
+    for name, mine, theirs in (("mean_speed", ms, ref["mean_speed"]), ("ke", ke, ref["ke"])):
+        m, t = float(np.mean(mine)), float(np.mean(theirs))
+        print(f"{name}: time average {m:.6g} vs reference {t:.6g} ({(m - t) / t * 100:+.3f} %)")
+        assert abs(m - t) <= 0.01 * abs(t)

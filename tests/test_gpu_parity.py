@@ -15,7 +15,7 @@ from parity import (check_fields, dam_break_scene, field_close, hash_cell_map, o
 pytestmark = pytest.mark.gpu
 
 
-def check_step(p, bx, pos, vel, bpos, delta, check_fields=True):
+def check_step(p, bx, pos, vel, bpos, delta, with_fields=True):
     got = run_one_step(p, bx, pos, vel, bpos, delta)
     ref, bs, bm = oracle_one_step(p, bx, pos, vel, bpos, delta)
     n = pos.shape[0]
@@ -39,7 +39,7 @@ def check_step(p, bx, pos, vel, bpos, delta, check_fields=True):
         ok, worst = field_close(got["boundary_mass"], bm)
         assert ok, f"boundary mass off by {worst:.3g} x tol"
     assert got["dt"][0] == np.float32(ref.dt_p) and got["dt"][1] == np.float32(ref.np_dt)
-    if not check_fields:
+    if not with_fields:
         return got, ref
     want = {"density": ref.rho, "pressure": ref.prs, "pressure_accel": ref.ap, "non_pressure_accel": ref.anp,
             "normal": ref.normal, "position": ref.pos, "velocity": ref.vel}
