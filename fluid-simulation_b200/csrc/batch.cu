@@ -71,6 +71,7 @@ struct BatchSim {
     DevBuf<u32> cstart, cend, mask;
     u32 table_size = 0;
     DevBuf<float> rho, prs, partials, metric_sums;
+    DevBuf<float2> dpr;
     DevBuf<float4> ap, normal, vlap, anp;
     DevBuf<DevState> st;
     DevBuf<DevScene> scenes;
@@ -107,7 +108,7 @@ struct BatchSim {
         a.boundary = HashView{btable.ptr, bcstart.ptr, bcend.ptr, btable_size ? btable_size - 1 : 0};
         a.mask = mask.ptr;
         a.mask_words = static_cast<u32>(mask_words);
-        a.rho = rho.ptr; a.prs = prs.ptr;
+        a.rho = rho.ptr; a.prs = prs.ptr; a.dpr = dpr.ptr;
         a.ap = ap.ptr; a.normal = normal.ptr; a.vlap = vlap.ptr; a.anp = anp.ptr;
         a.pos_out = pos_a.ptr; a.vel_out = vel_a.ptr;
         a.box = nullptr;
@@ -244,7 +245,7 @@ static void build_batch(BatchSim& B, const wcsph_params& p, const wcsph_batch_sc
     B.table_size = static_cast<u32>(std::max<u64>(std::bit_ceil(static_cast<u64>(n)) / 4, 64) * p.table_size_mult);
     B.table.alloc(B.table_size); B.cstart.alloc(B.table_size); B.cend.alloc(B.table_size);
     B.mask.alloc(n * static_cast<size_t>(B.mask_words));
-    B.rho.alloc(n); B.prs.alloc(n); B.ap.alloc(n); B.normal.alloc(n); B.vlap.alloc(n); B.anp.alloc(n);
+    B.rho.alloc(n); B.prs.alloc(n); B.dpr.alloc(n); B.ap.alloc(n); B.normal.alloc(n); B.vlap.alloc(n); B.anp.alloc(n);
     B.partials.alloc(2ull * (pass_grid(B.n, 2) + 1));
     B.metric_sums.alloc(2ull * S);
     B.st.alloc(1);

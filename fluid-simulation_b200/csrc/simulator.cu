@@ -148,7 +148,7 @@ void CUDASPHSimulator::allocate() {
     offsets_.alloc(SORT_DIGITS * 256);
     lookback_.alloc(static_cast<size_t>(SORT_DIGITS) * sort_tiles(n_) * 256);
     perm_.alloc(n); ckey_.alloc(n);
-    rho_.alloc(n); prs_.alloc(n);
+    rho_.alloc(n); prs_.alloc(n); dpr_.alloc(n);
     ap_.alloc(n); normal_.alloc(n); vlap_.alloc(n); anp_.alloc(n);
     st_.alloc(1); box_dev_.alloc(1); metrics_dev_.alloc(2);
     partials_.alloc(2ull * (pass_grid(n_, 2) + 1));
@@ -252,7 +252,7 @@ TravArgs CUDASPHSimulator::trav_args(float delta) {
     a.boundary = HashView{btable_.ptr, bcstart_.ptr, bcend_.ptr, btable_size_ ? btable_size_ - 1 : 0};
     a.mask = mask_.ptr;
     a.mask_words = static_cast<u32>(cfg_.mask_words);
-    a.rho = rho_.ptr; a.prs = prs_.ptr;
+    a.rho = rho_.ptr; a.prs = prs_.ptr; a.dpr = dpr_.ptr;
     a.ap = ap_.ptr; a.normal = normal_.ptr; a.vlap = vlap_.ptr; a.anp = anp_.ptr;
     a.pos_out = pos_a_.ptr; a.vel_out = vel_a_.ptr;
     a.box = box_dev_.ptr;

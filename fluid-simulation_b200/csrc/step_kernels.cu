@@ -25,17 +25,19 @@ __device__ __forceinline__ u32 warp_incl_scan(u32 v) {
     return v;
 }
 
-// What each pass stages per candidate and how many floats it accumulates
-// per (home, candidate-run) segment.
-//   sa: DENSITY / COUNT / FILL / ADJ_*: position
-//       FORCE:   (x, y, z, p_j / rho_j^2)    sb = (v_j, 1 / rho_j)
-//       SURFACE: (x, y, z, rho_j)            sb = (n_j, 0)
-//   cand: particle index of the candidate (passes that address j directly)
+// What each pass stages per candidate in shared memory and how many floats
+// it accumulates per (home, candidate-run) segment.
+//   DENSITY: positions as three float arrays (two candidates per packed
+//            FP32 step in the distance test)
+//   COUNT / FILL / ADJ_*: float4 positions and particle indices
+//   FORCE / SURFACE: particle indices only (they visit neighbours only and
+//            read the neighbour's fields through L1)
 template <int KIND>
 struct KindCfg {
-    static constexpr bool stage_b = KIND == PASS_FORCE || KIND == PASS_SURFACE;
-    static constexpr bool stage_j =
+    static constexpr bool soa = KIND == PASS_DENSITY;
+    static constexpr bool stage_sa =
         KIND == PASS_COUNT || KIND == PASS_FILL || KIND == PASS_ADJ_FORCE || KIND == PASS_ADJ_DENSITY;
+    static constexpr bool stage_j = KIND != PASS_DENSITY;
     static constexpr bool boundary =
         KIND == PASS_DENSITY || KIND == PASS_FORCE || KIND == PASS_ADJ_FORCE || KIND == PASS_ADJ_DENSITY;
     static constexpr int nf = (KIND == PASS_FORCE || KIND == PASS_ADJ_FORCE) ? 9
@@ -49,7 +51,9 @@ __host__ __device__ constexpr size_t align16(size_t b) { return (b + 15) & ~stat
 template <int KIND>
 struct WarpView {
     float4* sa;
-    float4* sb;
+    float* sx;
+    float* sy;
+    float* sz;
     u32* cand;
     u32* rstart;   // fluid cells: first particle
     u32* rpref;    // fluid cells: exclusive prefix of the cell sizes (+ total)
@@ -58,6 +62,7 @@ struct WarpView {
     u32* bpref;
     float* part;   // [SEG_SLOTS][nf] segment partials
     u32* aux;      // density: the block's bit matrix (cap words); others: row hit offsets
+    u32* hoff;     // row hit offsets (HOME_BLOCK + 1)
 };
 
 template <int KIND>
@@ -70,8 +75,10 @@ __host__ __device__ __forceinline__ size_t warp_smem_bytes(u32 cap, WarpView<KIN
         o += align16(bytes);
         return p;
     };
-    unsigned char* sa = take(16ull * cap);
-    unsigned char* sb = C::stage_b ? take(16ull * cap) : nullptr;
+    unsigned char* sa = C::stage_sa ? take(16ull * cap) : nullptr;
+    unsigned char* sx = C::soa ? take(4ull * cap) : nullptr;
+    unsigned char* sy = C::soa ? take(4ull * cap) : nullptr;
+    unsigned char* sz = C::soa ? take(4ull * cap) : nullptr;
     unsigned char* cand = C::stage_j ? take(4ull * cap) : nullptr;
     unsigned char* rstart = take(4ull * (MAX_RANGE_CELLS + 3));
     unsigned char* rpref = take(4ull * (MAX_RANGE_CELLS + 3));
@@ -82,10 +89,13 @@ __host__ __device__ __forceinline__ size_t warp_smem_bytes(u32 cap, WarpView<KIN
         bpref = take(4ull * (MAX_BOUNDARY_CELLS + 3));
     }
     unsigned char* part = take(4ull * SEG_SLOTS * C::nf);
-    unsigned char* aux = take(KIND == PASS_DENSITY ? 4ull * cap : 4ull * (HOME_BLOCK + 4));
+    unsigned char* aux = KIND == PASS_DENSITY ? take(4ull * cap) : nullptr;
+    unsigned char* hoff = take(4ull * (HOME_BLOCK + 4));
     if (v) {
         v->sa = reinterpret_cast<float4*>(sa);
-        v->sb = reinterpret_cast<float4*>(sb);
+        v->sx = reinterpret_cast<float*>(sx);
+        v->sy = reinterpret_cast<float*>(sy);
+        v->sz = reinterpret_cast<float*>(sz);
         v->cand = reinterpret_cast<u32*>(cand);
         v->rstart = reinterpret_cast<u32*>(rstart);
         v->rpref = reinterpret_cast<u32*>(rpref);
@@ -94,6 +104,7 @@ __host__ __device__ __forceinline__ size_t warp_smem_bytes(u32 cap, WarpView<KIN
         v->bpref = reinterpret_cast<u32*>(bpref);
         v->part = reinterpret_cast<float*>(part);
         v->aux = reinterpret_cast<u32*>(aux);
+        v->hoff = reinterpret_cast<u32*>(hoff);
     }
     return o;
 }
@@ -160,23 +171,31 @@ __device__ __forceinline__ void stage(const WarpView<KIND>& S, const TravArgs& a
         const u32 lo = range_of(S.rpref, ncell, m);
         const u32 j = S.rstart[lo] + (m - S.rpref[lo]);
         if constexpr (KindCfg<KIND>::stage_j) S.cand[ml] = j;
-        const float4 x = __ldg(a.pos + j);
-        if constexpr (KIND == PASS_FORCE) {
-            const float dj = __ldg(a.rho + j);
-            const float pj = __ldg(a.prs + j);
-            const float4 v = __ldg(a.vel + j);
-            S.sa[ml] = make_float4(x.x, x.y, x.z, pj / (dj * dj));
-            S.sb[ml] = make_float4(v.x, v.y, v.z, 1.f / dj);
-        } else if constexpr (KIND == PASS_SURFACE) {
-            const float dj = __ldg(a.rho + j);
-            const float4 nj = __ldg(a.normal + j);
-            S.sa[ml] = make_float4(x.x, x.y, x.z, dj);
-            S.sb[ml] = make_float4(nj.x, nj.y, nj.z, 0.f);
-        } else {
-            S.sa[ml] = x;
+        if constexpr (KindCfg<KIND>::stage_sa) S.sa[ml] = __ldg(a.pos + j);
+        if constexpr (KindCfg<KIND>::soa) {
+            const float4 x = __ldg(a.pos + j);
+            S.sx[ml] = x.x;
+            S.sy[ml] = x.y;
+            S.sz[ml] = x.z;
+        }
+    }
+    if constexpr (KindCfg<KIND>::soa) {
+        // an odd count is padded with a candidate at infinity (never a neighbour)
+        if ((len & 1u) && lane_id() == 0) {
+            S.sx[len] = __int_as_float(0x7f800000);
+            S.sy[len] = __int_as_float(0x7f800000);
+            S.sz[len] = __int_as_float(0x7f800000);
         }
     }
     __syncwarp();
+}
+
+// Position of staged candidate m.
+template <int KIND>
+__device__ __forceinline__ float4 cand_pos(const WarpView<KIND>& S, const TravArgs& a, u32 m) {
+    if constexpr (KindCfg<KIND>::stage_sa) return S.sa[m];
+    else if constexpr (KindCfg<KIND>::soa) return make_float4(S.sx[m], S.sy[m], S.sz[m], 0.f);
+    else return __ldg(a.pos + S.cand[m]);
 }
 
 __device__ __forceinline__ float4 f4(float x, float y, float z, float w = 0.f) { return make_float4(x, y, z, w); }
@@ -220,7 +239,12 @@ template <int KIND>
 __device__ __forceinline__ HomeData load_home(const TravArgs& a, u32 i) {
     HomeData H;
     H.x = __ldg(a.pos + i);
-    if constexpr (KIND == PASS_FORCE || KIND == PASS_ADJ_FORCE) {
+    if constexpr (KIND == PASS_FORCE) {
+        H.v = __ldg(a.vel + i);
+        H.prs = __ldg(a.prs + i);
+        H.dpi = __ldg(a.dpr + i).x;
+    }
+    if constexpr (KIND == PASS_ADJ_FORCE) {
         H.v = __ldg(a.vel + i);
         H.rho = __ldg(a.rho + i);
         H.prs = __ldg(a.prs + i);
@@ -279,31 +303,38 @@ template <int KIND>
 __device__ __forceinline__ void fluid_pair(float* v, const HomeData& H, const WarpView<KIND>& S, u32 m,
                                            float4 xj, float r2, const DevParams& P, const TravArgs& a) {
     const float rx = H.x.x - xj.x, ry = H.x.y - xj.y, rz = H.x.z - xj.z;
-    if constexpr (KIND == PASS_FORCE) {
+    if constexpr (KIND == PASS_DENSITY) {
+        float rinv;
+        v[0] += cubic_shape(q_of(r2, rinv, P));
+    } else if constexpr (KIND == PASS_FORCE) {
         // spiky_grad / cubic_grad (kernel.cuh:22-51) as coefficients of r
-        const float4 sbj = S.sb[m];
+        const u32 j = S.cand[m];
+        const float4 vj = __ldg(a.vel + j);
+        const float2 dj = __ldg(a.dpr + j);   // (p_j / rho_j^2, 1 / rho_j)
         float rinv;
         const float q = q_of(r2, rinv, P);
         const float t = 1.f - q;
         const float kr = (q >= 1.e-9f && q <= 1.f) ? rinv * P.inv_h : 0.f;
         const float sg = P.spiky_grad_factor * (t * t) * kr;
         const float cg = P.cubic_grad_factor * (q <= 0.5f ? q * (3.f * q - 2.f) : -(t * t)) * kr;
-        const float c = (H.dpi + xj.w) * sg;
+        const float c = (H.dpi + dj.x) * sg;
         v[0] -= c * rx; v[1] -= c * ry; v[2] -= c * rz;
-        const float cn = cg * sbj.w;
+        const float cn = cg * dj.y;
         v[3] += rx * cn; v[4] += ry * cn; v[5] += rz * cn;
-        const float vr = (H.v.x - sbj.x) * rx + (H.v.y - sbj.y) * ry + (H.v.z - sbj.z) * rz;
+        const float vr = (H.v.x - vj.x) * rx + (H.v.y - vj.y) * ry + (H.v.z - vj.z) * rz;
         const float s = __fdividef(vr * cn, r2 + P.visc_eps);
         v[6] += s * rx; v[7] += s * ry; v[8] += s * rz;
     } else if constexpr (KIND == PASS_SURFACE) {
         // cohesion (kernel.cuh:53-63); pairs closer than 1e-3 are skipped
-        const float4 nj = S.sb[m];
+        const u32 j = S.cand[m];
+        const float4 nj = __ldg(a.normal + j);
+        const float rho_j = __ldg(a.rho + j);
         float rinv;
         const float q = q_of(r2, rinv, P);
         const float t = 1.f - q;
         const float q3t3 = (q * q * q) * (t * t * t);
         const float coh = P.cohesion_factor * (q <= 0.5f ? 2.f * q3t3 - 1.f / 64.f : (q <= 1.f ? q3t3 : 0.f));
-        const float inv = r2 > 1e-6f ? __fdividef(1.f, H.rho + xj.w) : 0.f;
+        const float inv = r2 > 1e-6f ? __fdividef(1.f, H.rho + rho_j) : 0.f;
         const float cm = P.mass * coh * rinv;
         v[0] += (cm * rx + H.n.x - nj.x) * inv;
         v[1] += (cm * ry + H.n.y - nj.y) * inv;
@@ -425,9 +456,9 @@ __device__ __forceinline__ void combine(const float* part, float* res, bool acti
 
 // Fluid pairs rows [0, nh) x staged candidates [0, len) (candidate index
 // c0 + m), each tested against h^2 and the home particle itself (candidate
-// index self0 + row). BITS: the neighbour bits go to the block's bit matrix
-// in S.aux (row-major, row length len). Returns the run length.
-template <int KIND, bool BITS>
+// index self0 + row): the path of cells whose candidates exceed the bit
+// matrix capacity. Returns the run length.
+template <int KIND>
 __device__ __forceinline__ u32 fluid_pair_run(const WarpView<KIND>& S, const DevParams& P, const TravArgs& a,
                                               u32 nh, u32 len, u32 c0, u32 i0, u32 self0) {
     constexpr int NF = KindCfg<KIND>::nf;
@@ -444,25 +475,10 @@ __device__ __forceinline__ u32 fluid_pair_run(const WarpView<KIND>& S, const Dev
         float v[NF];
 #pragma unroll
         for (int f = 0; f < NF; ++f) v[f] = 0.f;
-        u32 wbits = 0;
         for (;;) {
-            const float4 xj = S.sa[m];
+            const float4 xj = cand_pos<KIND>(S, a, m);
             const float r2 = dist2(H.x, xj);
-            const bool nb = r2 <= P.h2 && m != self;
-            if constexpr (BITS) {
-                wbits |= static_cast<u32>(nb) << (p & 31u);
-                if ((p & 31u) == 31u || p + 1 == e) {
-                    if (wbits) atomicOr(S.aux + (p >> 5), wbits);
-                    wbits = 0;
-                }
-            }
-            if constexpr (KIND == PASS_DENSITY) {
-                float rinv;
-                const float w = cubic_shape(q_of(r2, rinv, P));
-                v[0] += nb ? w : 0.f;
-            } else {
-                if (nb) fluid_pair<KIND>(v, H, S, m, xj, r2, P, a);
-            }
+            if (r2 <= P.h2 && m != self) fluid_pair<KIND>(v, H, S, m, xj, r2, P, a);
             ++p;
             if (++m == len || p == e) {
                 store_partial<NF>(S.part, lane + k, v);
@@ -483,10 +499,14 @@ __device__ __forceinline__ u32 fluid_pair_run(const WarpView<KIND>& S, const Dev
 // Neighbour pairs of rows [0, nh) read from the block's bit matrix in
 // global memory (bits, row length M), split by hits. Returns the run length
 // (0: no hits) and, for row k = lane, its hit range [lo, hi).
-template <int KIND>
+template <int KIND, bool SHARED_BITS = false>
 __device__ __forceinline__ u32 fluid_hit_run(const WarpView<KIND>& S, const DevParams& P, const TravArgs& a,
                                              const u32* __restrict__ bits, u32 nh, u32 M, u32 i0, u32& lo,
                                              u32& hi) {
+    auto ld = [&](u32 w) -> u32 {
+        if constexpr (SHARED_BITS) return bits[w];
+        else return __ldg(bits + w);
+    };
     constexpr int NF = KindCfg<KIND>::nf;
     const u32 lane = lane_id();
     const u32 nwords = (nh * M + 31u) >> 5;
@@ -495,7 +515,7 @@ __device__ __forceinline__ u32 fluid_hit_run(const WarpView<KIND>& S, const DevP
         const u32 b0 = lane * M, b1 = b0 + M - 1;
         const u32 w0 = b0 >> 5, w1 = b1 >> 5;
         for (u32 w = w0; w <= w1; ++w) {
-            u32 x = __ldg(bits + w);
+            u32 x = ld(w);
             if (w == w0) x &= FULL << (b0 & 31u);
             if (w == w1) x &= FULL >> (31u - (b1 & 31u));
             cnt += __popc(x);
@@ -503,7 +523,7 @@ __device__ __forceinline__ u32 fluid_hit_run(const WarpView<KIND>& S, const DevP
     }
     const u32 incl = warp_incl_scan(cnt);
     const u32 total = __shfl_sync(FULL, incl, 31);
-    u32* hoff = S.aux;
+    u32* hoff = S.hoff;
     lo = incl - cnt;
     hi = incl;
     if (lane < nh) hoff[lane] = lo;
@@ -522,12 +542,12 @@ __device__ __forceinline__ u32 fluid_hit_run(const WarpView<KIND>& S, const DevP
         u32 r = h - hoff[k];
         u32 row0 = k * M;
         u32 wr = row0 >> 5;
-        u32 word = __ldg(bits + wr) & (FULL << (row0 & 31u));
+        u32 word = ld(wr) & (FULL << (row0 & 31u));
         for (;;) {
             const u32 pc = __popc(word);
             if (r < pc || wr + 1 >= nwords) break;
             r -= pc;
-            word = __ldg(bits + ++wr);
+            word = ld(++wr);
         }
         for (; r && word; --r) word &= word - 1;
         HomeData H = load_home<KIND>(a, i0 + k);
@@ -546,15 +566,66 @@ __device__ __forceinline__ u32 fluid_hit_run(const WarpView<KIND>& S, const DevP
                 H = load_home<KIND>(a, i0 + k);
             }
             const u32 m = p - row0;
-            const float4 xj = S.sa[m];
+            const float4 xj = cand_pos<KIND>(S, a, m);
             fluid_pair<KIND>(v, H, S, m, xj, dist2(H.x, xj), P, a);
             if (++h == e) break;
-            while (word == 0 && wr + 1 < nwords) word = __ldg(bits + ++wr);
+            while (word == 0 && wr + 1 < nwords) word = ld(++wr);
         }
         store_partial<NF>(S.part, lane + k, v);
     }
     __syncwarp();
     return c;
+}
+
+// Density pass, phase 1: distance test of rows [0, nh) x staged candidates
+// [0, len2) (len2 even; an odd count is padded with a candidate at
+// infinity). Each lane step tests two adjacent candidates in packed FP32
+// with the rounding of dist2() (x_i - x_j is formed as fma(x_j, -1, x_i),
+// the same single rounding), and the bits go to the block's bit matrix in
+// S.aux (row length len2). The home particle's own bit is set here and
+// cleared by the caller.
+__device__ __forceinline__ void density_test_run(const WarpView<PASS_DENSITY>& S, const DevParams& P,
+                                                 const TravArgs& a, u32 nh, u32 len2, u32 i0) {
+    const u32 lane = lane_id();
+    const u32 half = len2 >> 1;
+    const u32 total = nh * half;                 // candidate pairs
+    const u32 c = ((total + 31u) >> 5) | 1u;
+    u32 q = lane * c;
+    const u32 e = min(q + c, total);
+    if (q < e) {
+        u32 k = q / half;
+        u32 m2 = q - k * half;
+        const float2* sx = reinterpret_cast<const float2*>(S.sx);
+        const float2* sy = reinterpret_cast<const float2*>(S.sy);
+        const float2* sz = reinterpret_cast<const float2*>(S.sz);
+        const float2 neg = make_float2(-1.f, -1.f);
+        float4 h = __ldg(a.pos + i0 + k);
+        float2 X = make_float2(h.x, h.x), Y = make_float2(h.y, h.y), Z = make_float2(h.z, h.z);
+        u32 wbits = 0;
+        for (;;) {
+            const float2 dx = __ffma2_rn(sx[m2], neg, X);
+            const float2 dy = __ffma2_rn(sy[m2], neg, Y);
+            const float2 dz = __ffma2_rn(sz[m2], neg, Z);
+            const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
+            const u32 nb = (r2.x <= P.h2 ? 1u : 0u) | (r2.y <= P.h2 ? 2u : 0u);
+            wbits |= nb << ((q << 1) & 31u);
+            ++q;
+            if ((q & 15u) == 0u || q == e) {
+                if (wbits) atomicOr(S.aux + ((q - 1u) >> 4), wbits);
+                wbits = 0;
+            }
+            if (q == e) break;
+            if (++m2 == half) {
+                m2 = 0;
+                ++k;
+                h = __ldg(a.pos + i0 + k);
+                X = make_float2(h.x, h.x);
+                Y = make_float2(h.y, h.y);
+                Z = make_float2(h.z, h.z);
+            }
+        }
+    }
+    __syncwarp();
 }
 
 // Boundary pairs rows [0, nh) x expanded boundary candidates [0, len).
@@ -663,7 +734,8 @@ __global__ void __launch_bounds__(WPB * 32) cell_pass_kernel(const DevParams P, 
             const u32 home_start = S.rstart[qc];
             const u32 n_home = S.rpref[qc + 1] - S.rpref[qc];
             const u32 self_base = S.rpref[qc];   // candidate index of the first home particle
-            const bool masked = M <= cap;
+            const u32 Mrow = (M + 1u) & ~1u;       // bit-matrix row length (even)
+            const bool masked = Mrow <= cap;
 
             // boundary neighbour cells: union of the home particles' 3x3x3
             // boundary-cell neighbourhoods (cell size h, R = 1,
@@ -711,7 +783,7 @@ __global__ void __launch_bounds__(WPB * 32) cell_pass_kernel(const DevParams P, 
                 const u32 self0 = self_base + hb;
                 const bool act = lane < nh;
                 const u32 i = i0 + (act ? lane : 0u);
-                u32* const blk_bits = cell_bits + (hb >> 5) * M;   // row hb starts at bit hb * M
+                u32* const blk_bits = cell_bits + (hb >> 5) * Mrow;   // row hb starts at bit hb * Mrow
                 float res[NF], resb[NFB];
 #pragma unroll
                 for (int f = 0; f < NF; ++f) res[f] = 0.f;
@@ -725,7 +797,7 @@ __global__ void __launch_bounds__(WPB * 32) cell_pass_kernel(const DevParams P, 
                     if constexpr (KIND == PASS_FILL) wpos = act ? a.offsets[i] : 0u;
                     if (masked) {
                         if (act) {
-                            const u32 b0 = lane * M, b1 = b0 + M - 1;
+                            const u32 b0 = lane * Mrow, b1 = b0 + Mrow - 1;
                             for (u32 w = b0 >> 5; w <= (b1 >> 5); ++w) {
                                 u32 x = blk_bits[w];
                                 if (w == (b0 >> 5)) x &= FULL << (b0 & 31u);
@@ -765,32 +837,46 @@ __global__ void __launch_bounds__(WPB * 32) cell_pass_kernel(const DevParams P, 
                     }
                     continue;
                 } else if constexpr (KIND == PASS_DENSITY) {
-                    if (masked) {
-                        const u32 nwords = (nh * M + 31u) >> 5;
+                    // phase 1 tests every candidate and builds the bit matrix in shared
+                    // memory; phase 2 sums W over the neighbours only
+                    auto density_chunk = [&](u32 c0, u32 len, bool keep_bits) {
+                        const u32 len2 = (len + 1u) & ~1u;
+                        const u32 nwords = (nh * len2 + 31u) >> 5;
                         for (u32 w = lane; w < nwords; w += 32) S.aux[w] = 0u;
                         __syncwarp();
-                        const u32 c = fluid_pair_run<KIND, true>(S, P, a, nh, M, 0, i0, self0);
-                        combine<NF>(S.part, res, act, lane * M, lane * M + M, c);
-                        for (u32 w = lane; w < nwords; w += 32) blk_bits[w] = S.aux[w];
+                        density_test_run(S, P, a, nh, len2, i0);
+                        const u32 self = self0 + lane - c0;   // chunk index of the home particle itself
+                        if (act && self < len) {
+                            const u32 item = lane * len2 + self;
+                            atomicAnd(S.aux + (item >> 5), ~(1u << (item & 31u)));
+                        }
                         __syncwarp();
+                        u32 lo, hi;
+                        const u32 c = fluid_hit_run<KIND, true>(S, P, a, S.aux, nh, len2, i0, lo, hi);
+                        if (c) combine<NF>(S.part, res, act, lo, hi, c);
+                        if (keep_bits)
+                            for (u32 w = lane; w < nwords; w += 32) blk_bits[w] = S.aux[w];
+                        __syncwarp();
+                    };
+                    if (masked) {
+                        density_chunk(0, M, true);
                     } else {
                         for (u32 c0 = 0; c0 < M; c0 += cap) {
                             const u32 len = min(cap, M - c0);
                             stage<KIND>(S, a, ncell, c0, len);
-                            const u32 c = fluid_pair_run<KIND, false>(S, P, a, nh, len, c0, i0, self0);
-                            combine<NF>(S.part, res, act, lane * len, lane * len + len, c);
+                            density_chunk(c0, len, false);
                         }
                     }
                 } else {
                     if (masked) {
                         u32 lo, hi;
-                        const u32 c = fluid_hit_run<KIND>(S, P, a, blk_bits, nh, M, i0, lo, hi);
+                        const u32 c = fluid_hit_run<KIND>(S, P, a, blk_bits, nh, Mrow, i0, lo, hi);
                         if (c) combine<NF>(S.part, res, act, lo, hi, c);
                     } else {
                         for (u32 c0 = 0; c0 < M; c0 += cap) {
                             const u32 len = min(cap, M - c0);
                             stage<KIND>(S, a, ncell, c0, len);
-                            const u32 c = fluid_pair_run<KIND, false>(S, P, a, nh, len, c0, i0, self0);
+                            const u32 c = fluid_pair_run<KIND>(S, P, a, nh, len, c0, i0, self0);
                             combine<NF>(S.part, res, act, lane * len, lane * len + len, c);
                         }
                     }
@@ -810,8 +896,11 @@ __global__ void __launch_bounds__(WPB * 32) cell_pass_kernel(const DevParams P, 
                     if constexpr (KIND == PASS_DENSITY) {
                         // compute_density: (W(0) + sum W) * m, then + sum m_b W
                         const float rho = (P.w0 + P.cubic_factor * res[0]) * P.mass + P.cubic_factor * resb[0];
+                        const float prs = tait_pressure(rho, P);
                         a.rho[i] = rho;
-                        a.prs[i] = tait_pressure(rho, P);
+                        a.prs[i] = prs;
+                        // the force pass's per-neighbour factors p / rho^2 and 1 / rho
+                        a.dpr[i] = make_float2(prs / (rho * rho), 1.f / rho);
                     } else if constexpr (KIND == PASS_FORCE) {
                         // compute_pressure_accel_n_normal_with_boundary: m * sum_fluid, then
                         // the boundary term (compute_pressure_accel_n_normal.cu:346-364)

@@ -63,6 +63,7 @@ struct TravArgs {
     // fields
     float* rho;
     float* prs;
+    float2* dpr;              // (p / rho^2, 1 / rho), written by the density pass
     float4* ap;
     float4* normal;
     float4* vlap;
