@@ -13,6 +13,7 @@ constexpr u32 BCAND_CAP = 256;   // boundary candidates expanded per warp and ch
 constexpr u32 HOME_BLOCK = 32;   // home particles (bit-matrix rows) handled together
 constexpr u32 SEG_SLOTS = 64;    // segment partials, slot = lane + row (both < 32)
 
+
 __device__ __forceinline__ u32 lane_id() { return threadIdx.x & 31u; }
 
 __device__ __forceinline__ u32 warp_incl_scan(u32 v) {
@@ -27,8 +28,10 @@ __device__ __forceinline__ u32 warp_incl_scan(u32 v) {
 
 // What each pass stages per candidate in shared memory and how many floats
 // it accumulates per (home, candidate-run) segment.
-//   DENSITY: positions as three float arrays (two candidates per packed
-//            FP32 step in the distance test)
+//   DENSITY: positions in blocks of 16 candidate pairs, each pair as
+//            (x0,x1)(y0,y1)(z0,z1) float2s, one pad float2 per block (so that
+//            lanes on different blocks hit different banks); the distance
+//            test reads a pair per packed FP32 step
 //   COUNT / FILL / ADJ_*: float4 positions and particle indices
 //   FORCE / SURFACE: particle indices only (they visit neighbours only and
 //            read the neighbour's fields through L1)
@@ -43,17 +46,20 @@ struct KindCfg {
     static constexpr int nf = (KIND == PASS_FORCE || KIND == PASS_ADJ_FORCE) ? 9
                               : (KIND == PASS_SURFACE || KIND == PASS_ADJ_DENSITY) ? 3 : 1;
     static constexpr int nfb = KIND == PASS_ADJ_FORCE ? 4 : (KIND == PASS_DENSITY ? 1 : 3);
+    // neighbours fetched ahead per lane in the hit loops (bounded by registers)
+    static constexpr int hit_batch = (KIND == PASS_DENSITY || KIND == PASS_SURFACE) ? 4 : (KIND == PASS_FORCE ? 2 : 1);
 };
 
 __host__ __device__ constexpr size_t align16(size_t b) { return (b + 15) & ~static_cast<size_t>(15); }
+
+// float2 index of candidate pair pp in the density staging layout.
+__host__ __device__ __forceinline__ u32 pair_slot(u32 pp) { return 3u * pp + (pp >> 4); }
 
 // Per-warp shared memory, sized by the candidate capacity cap = 32 * mask_words.
 template <int KIND>
 struct WarpView {
     float4* sa;
-    float* sx;
-    float* sy;
-    float* sz;
+    float2* sp;    // density: candidate pair positions (pair_slot layout)
     u32* cand;
     u32* rstart;   // fluid cells: first particle
     u32* rpref;    // fluid cells: exclusive prefix of the cell sizes (+ total)
@@ -76,9 +82,7 @@ __host__ __device__ __forceinline__ size_t warp_smem_bytes(u32 cap, WarpView<KIN
         return p;
     };
     unsigned char* sa = C::stage_sa ? take(16ull * cap) : nullptr;
-    unsigned char* sx = C::soa ? take(4ull * cap) : nullptr;
-    unsigned char* sy = C::soa ? take(4ull * cap) : nullptr;
-    unsigned char* sz = C::soa ? take(4ull * cap) : nullptr;
+    unsigned char* sp = C::soa ? take(8ull * pair_slot(cap / 2)) : nullptr;
     unsigned char* cand = C::stage_j ? take(4ull * cap) : nullptr;
     unsigned char* rstart = take(4ull * (MAX_RANGE_CELLS + 3));
     unsigned char* rpref = take(4ull * (MAX_RANGE_CELLS + 3));
@@ -93,9 +97,7 @@ __host__ __device__ __forceinline__ size_t warp_smem_bytes(u32 cap, WarpView<KIN
     unsigned char* hoff = take(4ull * (HOME_BLOCK + 4));
     if (v) {
         v->sa = reinterpret_cast<float4*>(sa);
-        v->sx = reinterpret_cast<float*>(sx);
-        v->sy = reinterpret_cast<float*>(sy);
-        v->sz = reinterpret_cast<float*>(sz);
+        v->sp = reinterpret_cast<float2*>(sp);
         v->cand = reinterpret_cast<u32*>(cand);
         v->rstart = reinterpret_cast<u32*>(rstart);
         v->rpref = reinterpret_cast<u32*>(rpref);
@@ -161,41 +163,80 @@ __device__ __forceinline__ void expand(u32* cand, const u32* rstart, const u32* 
     __syncwarp();
 }
 
-// Like expand(), and stages the candidates' fields into shared memory with
-// lane-parallel loads (the pair loops then read shared memory only).
+// Stages candidates [c0, c0 + len) into shared memory: lane q walks cell q's
+// particles, so the loads are independent (no per-candidate search).
+// DENSITY pads the staged count up to a multiple of 32 with candidates at
+// infinity (never neighbours), so bit-matrix rows fill whole words.
+template <int KIND>
+__device__ __forceinline__ void soa_store(const WarpView<KIND>& S, u32 m, float4 x) {
+    float* f = reinterpret_cast<float*>(S.sp + pair_slot(m >> 1)) + (m & 1u);
+    f[0] = x.x;
+    f[2] = x.y;
+    f[4] = x.z;
+}
+
 template <int KIND>
 __device__ __forceinline__ void stage(const WarpView<KIND>& S, const TravArgs& a, u32 ncell, u32 c0, u32 len) {
     __syncwarp();
-    for (u32 ml = lane_id(); ml < len; ml += 32) {
-        const u32 m = c0 + ml;
-        const u32 lo = range_of(S.rpref, ncell, m);
-        const u32 j = S.rstart[lo] + (m - S.rpref[lo]);
-        if constexpr (KindCfg<KIND>::stage_j) S.cand[ml] = j;
-        if constexpr (KindCfg<KIND>::stage_sa) S.sa[ml] = __ldg(a.pos + j);
-        if constexpr (KindCfg<KIND>::soa) {
-            const float4 x = __ldg(a.pos + j);
-            S.sx[ml] = x.x;
-            S.sy[ml] = x.y;
-            S.sz[ml] = x.z;
+    const u32 lane = lane_id();
+    const u32 c1 = c0 + len;
+    for (u32 qb = 0; qb < ncell; qb += 32) {
+        const u32 q = qb + lane;
+        u32 lo = 0, hi = 0, src = 0;
+        if (q < ncell) {
+            const u32 b = S.rpref[q], e = S.rpref[q + 1];
+            lo = max(b, c0);
+            hi = min(e, c1);
+            src = S.rstart[q] + (lo - b);
+        }
+        for (u32 t = 0; lo + t < hi; ++t) {
+            const u32 j = src + t;
+            const u32 ml = lo + t - c0;
+            if constexpr (KindCfg<KIND>::stage_j) S.cand[ml] = j;
+            if constexpr (KindCfg<KIND>::stage_sa) S.sa[ml] = __ldg(a.pos + j);
+            if constexpr (KindCfg<KIND>::soa) soa_store(S, ml, __ldg(a.pos + j));
         }
     }
     if constexpr (KindCfg<KIND>::soa) {
-        // an odd count is padded with a candidate at infinity (never a neighbour)
-        if ((len & 1u) && lane_id() == 0) {
-            S.sx[len] = __int_as_float(0x7f800000);
-            S.sy[len] = __int_as_float(0x7f800000);
-            S.sz[len] = __int_as_float(0x7f800000);
-        }
+        const float inf = __int_as_float(0x7f800000);
+        for (u32 ml = len + lane; ml < ((len + 31u) & ~31u); ml += 32) soa_store(S, ml, make_float4(inf, inf, inf, 0.f));
     }
     __syncwarp();
 }
 
-// Position of staged candidate m.
+// A neighbour's data, fetched ahead of the pair arithmetic so that several
+// neighbours' loads are in flight at once.
+//   x: position; FORCE: b = (v_j, 1 / rho_j), c = p_j / rho_j^2;
+//   SURFACE: b = n_j, c = rho_j; j: particle index (passes that address j).
+struct Nbr {
+    float4 x, b;
+    float c;
+    u32 j;
+};
+
 template <int KIND>
-__device__ __forceinline__ float4 cand_pos(const WarpView<KIND>& S, const TravArgs& a, u32 m) {
-    if constexpr (KindCfg<KIND>::stage_sa) return S.sa[m];
-    else if constexpr (KindCfg<KIND>::soa) return make_float4(S.sx[m], S.sy[m], S.sz[m], 0.f);
-    else return __ldg(a.pos + S.cand[m]);
+__device__ __forceinline__ Nbr fetch(const WarpView<KIND>& S, const TravArgs& a, u32 m) {
+    Nbr d;
+    if constexpr (KindCfg<KIND>::soa) {
+        const float* f = reinterpret_cast<const float*>(S.sp + pair_slot(m >> 1)) + (m & 1u);
+        d.x = make_float4(f[0], f[2], f[4], 0.f);
+    } else if constexpr (KIND == PASS_FORCE) {
+        d.j = S.cand[m];
+        d.x = __ldg(a.pos + d.j);
+        d.b = __ldg(a.vel + d.j);
+        const float2 q = __ldg(a.dpr + d.j);
+        d.b.w = q.y;
+        d.c = q.x;
+    } else if constexpr (KIND == PASS_SURFACE) {
+        d.j = S.cand[m];
+        d.x = __ldg(a.pos + d.j);
+        d.b = __ldg(a.normal + d.j);
+        d.c = __ldg(a.rho + d.j);
+    } else {
+        d.j = S.cand[m];
+        d.x = S.sa[m];
+    }
+    return d;
 }
 
 __device__ __forceinline__ float4 f4(float x, float y, float z, float w = 0.f) { return make_float4(x, y, z, w); }
@@ -300,35 +341,31 @@ __device__ __forceinline__ float q_of(float r2, float& rinv, const DevParams& P)
 //   ADJ_FORCE   v0..2 = dL/dx_i, v3..5 = dL/dv_i, v6 = pressure-coefficient term, v7 = viscosity rho term
 //   ADJ_DENSITY v0..2 = dL/dx_i
 template <int KIND>
-__device__ __forceinline__ void fluid_pair(float* v, const HomeData& H, const WarpView<KIND>& S, u32 m,
-                                           float4 xj, float r2, const DevParams& P, const TravArgs& a) {
-    const float rx = H.x.x - xj.x, ry = H.x.y - xj.y, rz = H.x.z - xj.z;
+__device__ __forceinline__ void fluid_pair(float* v, const HomeData& H, const Nbr& d, float r2, const DevParams& P,
+                                           const TravArgs& a) {
+    const float rx = H.x.x - d.x.x, ry = H.x.y - d.x.y, rz = H.x.z - d.x.z;
     if constexpr (KIND == PASS_DENSITY) {
         float rinv;
         v[0] += cubic_shape(q_of(r2, rinv, P));
     } else if constexpr (KIND == PASS_FORCE) {
         // spiky_grad / cubic_grad (kernel.cuh:22-51) as coefficients of r
-        const u32 j = S.cand[m];
-        const float4 vj = __ldg(a.vel + j);
-        const float2 dj = __ldg(a.dpr + j);   // (p_j / rho_j^2, 1 / rho_j)
         float rinv;
         const float q = q_of(r2, rinv, P);
         const float t = 1.f - q;
         const float kr = (q >= 1.e-9f && q <= 1.f) ? rinv * P.inv_h : 0.f;
         const float sg = P.spiky_grad_factor * (t * t) * kr;
         const float cg = P.cubic_grad_factor * (q <= 0.5f ? q * (3.f * q - 2.f) : -(t * t)) * kr;
-        const float c = (H.dpi + dj.x) * sg;
+        const float c = (H.dpi + d.c) * sg;
         v[0] -= c * rx; v[1] -= c * ry; v[2] -= c * rz;
-        const float cn = cg * dj.y;
+        const float cn = cg * d.b.w;
         v[3] += rx * cn; v[4] += ry * cn; v[5] += rz * cn;
-        const float vr = (H.v.x - vj.x) * rx + (H.v.y - vj.y) * ry + (H.v.z - vj.z) * rz;
+        const float vr = (H.v.x - d.b.x) * rx + (H.v.y - d.b.y) * ry + (H.v.z - d.b.z) * rz;
         const float s = __fdividef(vr * cn, r2 + P.visc_eps);
         v[6] += s * rx; v[7] += s * ry; v[8] += s * rz;
     } else if constexpr (KIND == PASS_SURFACE) {
         // cohesion (kernel.cuh:53-63); pairs closer than 1e-3 are skipped
-        const u32 j = S.cand[m];
-        const float4 nj = __ldg(a.normal + j);
-        const float rho_j = __ldg(a.rho + j);
+        const float4 nj = d.b;
+        const float rho_j = d.c;
         float rinv;
         const float q = q_of(r2, rinv, P);
         const float t = 1.f - q;
@@ -341,7 +378,7 @@ __device__ __forceinline__ void fluid_pair(float* v, const HomeData& H, const Wa
         v[2] += (cm * rz + H.n.z - nj.z) * inv;
     } else if constexpr (KIND == PASS_ADJ_FORCE) {
         // pressure: a_i = -m sum_j A_ij F(r_ij), F(r) = g_s(|r|) r, A_ij = p_i/rho_i^2 + p_j/rho_j^2
-        const u32 j = S.cand[m];
+        const u32 j = d.j;
         const float rl = sqrtf(r2);
         const float q = rl * P.inv_h;
         const float dj = __ldg(a.rho + j);
@@ -383,7 +420,7 @@ __device__ __forceinline__ void fluid_pair(float* v, const HomeData& H, const Wa
                 sj * (uz * G * wjr + ur * G * wj.z + ur * wjr * Gp * rz);
     } else if constexpr (KIND == PASS_ADJ_DENSITY) {
         // rho_i = m (W(0) + sum_j W(|r_ij|)): dW/dx_i = g_c r_ij, shared by rho_i and rho_j
-        const u32 j = S.cand[m];
+        const u32 j = d.j;
         const float q = sqrtf(r2) * P.inv_h;
         const float rb = __ldg(a.adj_rhobar + j);
         const float c = P.mass * cubic_grad(q, P) * (H.rb + rb);
@@ -476,9 +513,9 @@ __device__ __forceinline__ u32 fluid_pair_run(const WarpView<KIND>& S, const Dev
 #pragma unroll
         for (int f = 0; f < NF; ++f) v[f] = 0.f;
         for (;;) {
-            const float4 xj = cand_pos<KIND>(S, a, m);
-            const float r2 = dist2(H.x, xj);
-            if (r2 <= P.h2 && m != self) fluid_pair<KIND>(v, H, S, m, xj, r2, P, a);
+            const Nbr d = fetch<KIND>(S, a, m);
+            const float r2 = dist2(H.x, d.x);
+            if (r2 <= P.h2 && m != self) fluid_pair<KIND>(v, H, d, r2, P, a);
             ++p;
             if (++m == len || p == e) {
                 store_partial<NF>(S.part, lane + k, v);
@@ -550,80 +587,82 @@ __device__ __forceinline__ u32 fluid_hit_run(const WarpView<KIND>& S, const DevP
             word = ld(++wr);
         }
         for (; r && word; --r) word &= word - 1;
-        HomeData H = load_home<KIND>(a, i0 + k);
+        // the lane's hits, HIT_BATCH at a time: the bit walk first, then every
+        // neighbour's loads, then the arithmetic
+        constexpr int G = KindCfg<KIND>::hit_batch;
+        u32 kc = k;                  // row of the segment being accumulated
+        HomeData H = load_home<KIND>(a, i0 + kc);
         float v[NF];
 #pragma unroll
         for (int f = 0; f < NF; ++f) v[f] = 0.f;
-        while (word) {
-            const u32 b = __ffs(word) - 1;
-            word &= word - 1;
-            const u32 p = (wr << 5) + b;
-            if (p >= row0 + M) {
-                store_partial<NF>(S.part, lane + k, v);
+        while (h < e) {
+            u32 mm[G], kk[G];
+            u32 cnt = 0;
 #pragma unroll
-                for (int f = 0; f < NF; ++f) v[f] = 0.f;
-                do { ++k; row0 += M; } while (p >= row0 + M);
-                H = load_home<KIND>(a, i0 + k);
+            for (int t = 0; t < G; ++t) {
+                if (h < e) {
+                    while (word == 0 && wr + 1 < nwords) word = ld(++wr);
+                    if (word == 0) { h = e; break; }   // unreachable with consistent bits
+                    const u32 b = __ffs(word) - 1;
+                    word &= word - 1;
+                    const u32 p = (wr << 5) + b;
+                    while (p >= row0 + M) { ++k; row0 += M; }
+                    mm[t] = p - row0;
+                    kk[t] = k;
+                    ++cnt;
+                    ++h;
+                }
             }
-            const u32 m = p - row0;
-            const float4 xj = cand_pos<KIND>(S, a, m);
-            fluid_pair<KIND>(v, H, S, m, xj, dist2(H.x, xj), P, a);
-            if (++h == e) break;
-            while (word == 0 && wr + 1 < nwords) word = ld(++wr);
+            Nbr d[G];
+#pragma unroll
+            for (int t = 0; t < G; ++t)
+                if (t < cnt) d[t] = fetch<KIND>(S, a, mm[t]);
+#pragma unroll
+            for (int t = 0; t < G; ++t) {
+                if (t < cnt) {
+                    if (kk[t] != kc) {
+                        store_partial<NF>(S.part, lane + kc, v);
+#pragma unroll
+                        for (int f = 0; f < NF; ++f) v[f] = 0.f;
+                        kc = kk[t];
+                        H = load_home<KIND>(a, i0 + kc);
+                    }
+                    fluid_pair<KIND>(v, H, d[t], dist2(H.x, d[t].x), P, a);
+                }
+            }
         }
-        store_partial<NF>(S.part, lane + k, v);
+        store_partial<NF>(S.part, lane + kc, v);
     }
     __syncwarp();
     return c;
 }
 
 // Density pass, phase 1: distance test of rows [0, nh) x staged candidates
-// [0, len2) (len2 even; an odd count is padded with a candidate at
-// infinity). Each lane step tests two adjacent candidates in packed FP32
-// with the rounding of dist2() (x_i - x_j is formed as fma(x_j, -1, x_i),
-// the same single rounding), and the bits go to the block's bit matrix in
-// S.aux (row length len2). The home particle's own bit is set here and
-// cleared by the caller.
-__device__ __forceinline__ void density_test_run(const WarpView<PASS_DENSITY>& S, const DevParams& P,
-                                                 const TravArgs& a, u32 nh, u32 len2, u32 i0) {
-    const u32 lane = lane_id();
-    const u32 half = len2 >> 1;
-    const u32 total = nh * half;                 // candidate pairs
-    const u32 c = ((total + 31u) >> 5) | 1u;
-    u32 q = lane * c;
-    const u32 e = min(q + c, total);
-    if (q < e) {
-        u32 k = q / half;
-        u32 m2 = q - k * half;
-        const float2* sx = reinterpret_cast<const float2*>(S.sx);
-        const float2* sy = reinterpret_cast<const float2*>(S.sy);
-        const float2* sz = reinterpret_cast<const float2*>(S.sz);
-        const float2 neg = make_float2(-1.f, -1.f);
-        float4 h = __ldg(a.pos + i0 + k);
-        float2 X = make_float2(h.x, h.x), Y = make_float2(h.y, h.y), Z = make_float2(h.z, h.z);
-        u32 wbits = 0;
-        for (;;) {
-            const float2 dx = __ffma2_rn(sx[m2], neg, X);
-            const float2 dy = __ffma2_rn(sy[m2], neg, Y);
-            const float2 dz = __ffma2_rn(sz[m2], neg, Z);
+// [0, 32 wpr) (the padding candidates lie at infinity). One lane builds one
+// word of the bit matrix (row-major, wpr words per row): 16 candidate pairs,
+// unrolled, each tested in packed FP32 with the rounding of dist2()
+// (x_i - x_j is formed as fma(x_j, -1, x_i), the same single rounding).
+// The home particle's own bit is set here and cleared by the caller.
+__device__ __forceinline__ void density_test_words(const WarpView<PASS_DENSITY>& S, const DevParams& P,
+                                                   const TravArgs& a, u32 nh, u32 wpr, u32 i0) {
+    const u32 nwords = nh * wpr;
+    const float2 neg = make_float2(-1.f, -1.f);
+    for (u32 w = lane_id(); w < nwords; w += 32) {
+        const u32 k = w / wpr;
+        const u32 wi = w - k * wpr;
+        const float4 h = __ldg(a.pos + i0 + k);
+        const float2 X = make_float2(h.x, h.x), Y = make_float2(h.y, h.y), Z = make_float2(h.z, h.z);
+        const float2* base = S.sp + pair_slot(wi * 16u);
+        u32 bits = 0;
+#pragma unroll
+        for (int t = 0; t < 16; ++t) {
+            const float2 dx = __ffma2_rn(base[3 * t], neg, X);
+            const float2 dy = __ffma2_rn(base[3 * t + 1], neg, Y);
+            const float2 dz = __ffma2_rn(base[3 * t + 2], neg, Z);
             const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
-            const u32 nb = (r2.x <= P.h2 ? 1u : 0u) | (r2.y <= P.h2 ? 2u : 0u);
-            wbits |= nb << ((q << 1) & 31u);
-            ++q;
-            if ((q & 15u) == 0u || q == e) {
-                if (wbits) atomicOr(S.aux + ((q - 1u) >> 4), wbits);
-                wbits = 0;
-            }
-            if (q == e) break;
-            if (++m2 == half) {
-                m2 = 0;
-                ++k;
-                h = __ldg(a.pos + i0 + k);
-                X = make_float2(h.x, h.x);
-                Y = make_float2(h.y, h.y);
-                Z = make_float2(h.z, h.z);
-            }
+            bits |= (r2.x <= P.h2 ? 1u << (2 * t) : 0u) | (r2.y <= P.h2 ? 2u << (2 * t) : 0u);
         }
+        S.aux[w] = bits;
     }
     __syncwarp();
 }
@@ -667,7 +706,7 @@ __device__ __forceinline__ u32 boundary_pair_run(const WarpView<KIND>& S, const 
 }
 
 template <int KIND, int WPB, bool BATCH>
-__global__ void __launch_bounds__(WPB * 32) cell_pass_kernel(const DevParams P, const TravArgs a) {
+__global__ void __launch_bounds__(WPB * 32, 24 / WPB) cell_pass_kernel(const DevParams P, const TravArgs a) {
     using C = KindCfg<KIND>;
     constexpr int NF = C::nf;
     constexpr int NFB = C::nfb;
@@ -734,7 +773,7 @@ __global__ void __launch_bounds__(WPB * 32) cell_pass_kernel(const DevParams P, 
             const u32 home_start = S.rstart[qc];
             const u32 n_home = S.rpref[qc + 1] - S.rpref[qc];
             const u32 self_base = S.rpref[qc];   // candidate index of the first home particle
-            const u32 Mrow = (M + 1u) & ~1u;       // bit-matrix row length (even)
+            const u32 Mrow = (M + 31u) & ~31u;     // bit-matrix row length (whole words)
             const bool masked = Mrow <= cap;
 
             // boundary neighbour cells: union of the home particles' 3x3x3
@@ -840,19 +879,18 @@ __global__ void __launch_bounds__(WPB * 32) cell_pass_kernel(const DevParams P, 
                     // phase 1 tests every candidate and builds the bit matrix in shared
                     // memory; phase 2 sums W over the neighbours only
                     auto density_chunk = [&](u32 c0, u32 len, bool keep_bits) {
-                        const u32 len2 = (len + 1u) & ~1u;
-                        const u32 nwords = (nh * len2 + 31u) >> 5;
-                        for (u32 w = lane; w < nwords; w += 32) S.aux[w] = 0u;
-                        __syncwarp();
-                        density_test_run(S, P, a, nh, len2, i0);
+                        const u32 wpr = (len + 31u) >> 5;
+                        const u32 len32 = wpr << 5;
+                        const u32 nwords = nh * wpr;
+                        density_test_words(S, P, a, nh, wpr, i0);
                         const u32 self = self0 + lane - c0;   // chunk index of the home particle itself
                         if (act && self < len) {
-                            const u32 item = lane * len2 + self;
+                            const u32 item = lane * len32 + self;
                             atomicAnd(S.aux + (item >> 5), ~(1u << (item & 31u)));
                         }
                         __syncwarp();
                         u32 lo, hi;
-                        const u32 c = fluid_hit_run<KIND, true>(S, P, a, S.aux, nh, len2, i0, lo, hi);
+                        const u32 c = fluid_hit_run<KIND, true>(S, P, a, S.aux, nh, len32, i0, lo, hi);
                         if (c) combine<NF>(S.part, res, act, lo, hi, c);
                         if (keep_bits)
                             for (u32 w = lane; w < nwords; w += 32) blk_bits[w] = S.aux[w];
