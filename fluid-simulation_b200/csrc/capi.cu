@@ -6,6 +6,7 @@
 #include "batch.cuh"
 #include "scene_io.h"
 #include "simulator.cuh"
+#include "static_sort.cuh"
 
 struct wcsph_ctx {
     std::unique_ptr<wcsph::CUDASPHSimulator> sim;
@@ -353,6 +354,15 @@ int wcsph_rollout_forward(wcsph_ctx* ctx, int steps, float dt, int checkpoint_ev
 int wcsph_rollout_backward(wcsph_ctx* ctx, float* grad_v0, float* grad_viscosity, float* grad_stiffness) {
     CHECK_CTX(ctx);
     return guarded(ctx, [&] { ctx->sim->rollout_backward(grad_v0, grad_viscosity, grad_stiffness); });
+}
+
+// ---- allocation-free key sort ------------------------------------------------
+// No counterpart in the reference; for callers that cannot allocate device
+// memory while they run (see include/wcsph.h). Errors go to wcsph_last_error(NULL).
+int wcsph_sort_keys_static(const uint64_t* keys, uint32_t n, uint32_t* perm, void* stream) {
+    return guarded(nullptr, [&] {
+        wcsph::static_sort_permutation(keys, n, perm, static_cast<cudaStream_t>(stream));
+    });
 }
 
 }  // extern "C"

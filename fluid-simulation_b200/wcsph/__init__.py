@@ -182,6 +182,7 @@ def load_library(path: str | os.PathLike | None = None) -> C.CDLL:
         "wcsph_batch_last_error": (C.c_char_p, [vp]),
         "wcsph_rollout_forward": (C.c_int, [vp, C.c_int, C.c_float, C.c_int, f, f]),
         "wcsph_rollout_backward": (C.c_int, [vp, f, f, f]),
+        "wcsph_sort_keys_static": (C.c_int, [vp, C.c_uint32, vp, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -335,6 +336,18 @@ def _check(status: int, ctx, lib=None):
                   ERR_SNAPSHOT_TRUNCATED) or (status == ERR_IO and "Snapshot" in msg):
         raise SnapshotError(status, msg)
     raise WcsphError(status, msg or lib.wcsph_status_string(status).decode())
+
+
+STATIC_SORT_MAX_KEYS = 65536
+
+
+def sort_keys_static(keys_ptr: int, n: int, perm_ptr: int, stream: int | None = None) -> None:
+    """Stable sort permutation of n device-resident uint64 keys into the device
+    uint32 array at perm_ptr, without allocating device memory (for callers
+    that cannot allocate while they run; see wcsph_sort_keys_static in
+    include/wcsph.h). Enqueued on `stream` (a cudaStream_t handle, None = the
+    default stream); the call does not wait for the GPU."""
+    _check(load_library().wcsph_sort_keys_static(keys_ptr, n, perm_ptr, stream), None)
 
 
 def snapshot_read(path, app_name: str, fluid_n: int):

@@ -325,6 +325,32 @@ int wcsph_rollout_forward(wcsph_ctx* ctx, int steps, float dt, int checkpoint_ev
 int wcsph_rollout_backward(wcsph_ctx* ctx, float* grad_v0, float* grad_viscosity,
                            float* grad_stiffness);
 
+/* ---- allocation-free key sort ---------------------------------------------
+ * No counterpart in the reference (its sort is thrust::sort_by_key, which
+ * allocates temporary storage on every call).
+ *
+ * For callers that cannot call cudaMalloc/cudaFree while they run: a render
+ * or control loop that must not take the device-wide synchronisation that
+ * freeing device memory implies, or a host that works inside a device memory
+ * budget reserved up front. Writes to perm (device array of n uint32) the
+ * stable sort permutation of the n device-resident 64-bit keys (perm[i] = index
+ * of the key of rank i, equal keys in input order): the same permutation the
+ * step's sort produces (WCSPH_FIELD_PERMUTATION for WCSPH_FIELD_MORTON_KEYS).
+ * keys is only read. Nothing is allocated: the scratch is a device array of the
+ * library image, about 1.8 MiB, that every GPU loading the library holds until
+ * the process exits.
+ *   - n above WCSPH_STATIC_SORT_MAX_KEYS returns WCSPH_ERR_INVALID_ARGUMENT
+ *     (text via wcsph_last_error(NULL)); n == 0 does nothing.
+ *   - The work is enqueued on `stream` (a cudaStream_t; NULL = the default
+ *     stream) of the current device and the call returns without waiting.
+ *   - The first call on a device looks up the scratch's device address (set-up
+ *     done once per device); make that first call before any stream capture.
+ *   - Every call on a device shares the one scratch: calls whose work overlaps
+ *     on the GPU (other streams, other host threads) race and corrupt each
+ *     other's results. Order them on one stream or synchronise between them. */
+#define WCSPH_STATIC_SORT_MAX_KEYS 65536u
+int wcsph_sort_keys_static(const uint64_t* keys, uint32_t n, uint32_t* perm, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
