@@ -80,7 +80,7 @@ struct BatchSim {
     DevBuf<u64> btable, bckey;
     DevBuf<u32> bcstart, bcend;
     u32 btable_size = 0;
-    int mask_words = 16;
+    int mask_words = 10;
 
     cudaGraphExec_t graph = nullptr;
     float graph_delta = -1.f;
@@ -137,9 +137,9 @@ struct BatchSim {
                              vel_b.ptr, perm.ptr, ckey.ptr, table.ptr, cstart.ptr, cend.ptr, table_size - 1, st.ptr,
                              stream, scene_a.ptr);
         const TravArgs a = args(delta);
-        launch_pass(PASS_DENSITY, dp, a, stream, 4, true);
-        launch_pass(PASS_FORCE, dp, a, stream, 4, true);
-        launch_pass(PASS_SURFACE, dp, a, stream, 4, true);
+        launch_pass(PASS_DENSITY, dp, a, stream, 2, true);
+        launch_pass(PASS_FORCE, dp, a, stream, 2, true);
+        launch_pass(PASS_SURFACE, dp, a, stream, 2, true);
     }
 
     void step_n(int k, float delta) {

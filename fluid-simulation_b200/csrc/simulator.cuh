@@ -71,10 +71,10 @@ float metric_mass(const wcsph_params& p);
 
 // Tunable launch configuration of the step (the autotuner's search space).
 struct StepConfig {
-    int warps_density = 4;
-    int warps_force = 4;
-    int warps_surface = 4;
-    int mask_words = 16;        // neighbour bitmask words per particle (cap = 32*words)
+    int warps_density = 2;
+    int warps_force = 2;
+    int warps_surface = 2;
+    int mask_words = 10;        // neighbour bit-matrix words per particle (cap = 32*words)
     float cell_size_mult = 1.f;
     uint32_t table_size_mult = 1;
     bool operator==(const StepConfig&) const = default;

@@ -46,8 +46,6 @@ struct KindCfg {
     static constexpr int nf = (KIND == PASS_FORCE || KIND == PASS_ADJ_FORCE) ? 9
                               : (KIND == PASS_SURFACE || KIND == PASS_ADJ_DENSITY) ? 3 : 1;
     static constexpr int nfb = KIND == PASS_ADJ_FORCE ? 4 : (KIND == PASS_DENSITY ? 1 : 3);
-    // neighbours fetched ahead per lane in the hit loops (bounded by registers)
-    static constexpr int hit_batch = (KIND == PASS_DENSITY || KIND == PASS_SURFACE) ? 4 : (KIND == PASS_FORCE ? 2 : 1);
 };
 
 __host__ __device__ constexpr size_t align16(size_t b) { return (b + 15) & ~static_cast<size_t>(15); }
@@ -204,8 +202,7 @@ __device__ __forceinline__ void stage(const WarpView<KIND>& S, const TravArgs& a
     __syncwarp();
 }
 
-// A neighbour's data, fetched ahead of the pair arithmetic so that several
-// neighbours' loads are in flight at once.
+// A neighbour's data as the pair arithmetic reads it.
 //   x: position; FORCE: b = (v_j, 1 / rho_j), c = p_j / rho_j^2;
 //   SURFACE: b = n_j, c = rho_j; j: particle index (passes that address j).
 struct Nbr {
@@ -587,51 +584,27 @@ __device__ __forceinline__ u32 fluid_hit_run(const WarpView<KIND>& S, const DevP
             word = ld(++wr);
         }
         for (; r && word; --r) word &= word - 1;
-        // the lane's hits, HIT_BATCH at a time: the bit walk first, then every
-        // neighbour's loads, then the arithmetic
-        constexpr int G = KindCfg<KIND>::hit_batch;
-        u32 kc = k;                  // row of the segment being accumulated
-        HomeData H = load_home<KIND>(a, i0 + kc);
+        HomeData H = load_home<KIND>(a, i0 + k);
         float v[NF];
 #pragma unroll
         for (int f = 0; f < NF; ++f) v[f] = 0.f;
-        while (h < e) {
-            u32 mm[G], kk[G];
-            u32 cnt = 0;
+        while (word) {
+            const u32 b = __ffs(word) - 1;
+            word &= word - 1;
+            const u32 p = (wr << 5) + b;
+            if (p >= row0 + M) {   // the walk crossed into a later row: close row k's segment
+                store_partial<NF>(S.part, lane + k, v);
 #pragma unroll
-            for (int t = 0; t < G; ++t) {
-                if (h < e) {
-                    while (word == 0 && wr + 1 < nwords) word = ld(++wr);
-                    if (word == 0) { h = e; break; }   // unreachable with consistent bits
-                    const u32 b = __ffs(word) - 1;
-                    word &= word - 1;
-                    const u32 p = (wr << 5) + b;
-                    while (p >= row0 + M) { ++k; row0 += M; }
-                    mm[t] = p - row0;
-                    kk[t] = k;
-                    ++cnt;
-                    ++h;
-                }
+                for (int f = 0; f < NF; ++f) v[f] = 0.f;
+                do { ++k; row0 += M; } while (p >= row0 + M);
+                H = load_home<KIND>(a, i0 + k);
             }
-            Nbr d[G];
-#pragma unroll
-            for (int t = 0; t < G; ++t)
-                if (t < cnt) d[t] = fetch<KIND>(S, a, mm[t]);
-#pragma unroll
-            for (int t = 0; t < G; ++t) {
-                if (t < cnt) {
-                    if (kk[t] != kc) {
-                        store_partial<NF>(S.part, lane + kc, v);
-#pragma unroll
-                        for (int f = 0; f < NF; ++f) v[f] = 0.f;
-                        kc = kk[t];
-                        H = load_home<KIND>(a, i0 + kc);
-                    }
-                    fluid_pair<KIND>(v, H, d[t], dist2(H.x, d[t].x), P, a);
-                }
-            }
+            const Nbr d = fetch<KIND>(S, a, p - row0);
+            fluid_pair<KIND>(v, H, d, dist2(H.x, d.x), P, a);
+            if (++h == e) break;
+            while (word == 0 && wr + 1 < nwords) word = ld(++wr);
         }
-        store_partial<NF>(S.part, lane + kc, v);
+        store_partial<NF>(S.part, lane + k, v);
     }
     __syncwarp();
     return c;

@@ -11,7 +11,7 @@ namespace wcsph {
 
 namespace {
 const int kWarps[] = {2, 4, 8};
-const int kMaskWords[] = {8, 12, 16};
+const int kMaskWords[] = {8, 10, 12, 16};
 const double kCellMult[] = {0.5, 2. / 3., 1., 1.5, 2.};  // step_tuner.cuh:88
 const uint32_t kTableMult[] = {1, 2, 4, 8, 16, 32};      // step_tuner.cuh:251-256
 
@@ -219,7 +219,7 @@ int Tuner::next_candidate() {
         case 0: shift(c.warps_density, kWarps, 3); break;
         case 1: shift(c.warps_force, kWarps, 3); break;
         case 2: shift(c.warps_surface, kWarps, 3); break;
-        case 3: shift(c.mask_words, kMaskWords, 3); break;
+        case 3: shift(c.mask_words, kMaskWords, 4); break;
         case 4: {
             int idx = 0;
             for (int k = 0; k < 5; ++k) if (static_cast<float>(kCellMult[k]) == c.cell_size_mult) idx = k;
