@@ -6,10 +6,11 @@
 // Positions, velocities and particle ids are checkpointed every K steps.
 //
 // Backward, per segment (last first): the segment is re-run from its
-// checkpoint keeping each step's input state; then for each step in reverse
-// the neighbourhood search, density and force passes are recomputed from that
-// input (the neighbour sets are recomputed, not stored) and the adjoint
-// kernels run:
+// checkpoint, each step with its own buffer set swapped in (sorted state,
+// permutation, hash and cell ranges, neighbour bit matrix, density, pressure,
+// accelerations), so every step's neighbour sets are recomputed from the
+// checkpoint, not stored across the rollout. Then for each step in reverse,
+// with that step's set swapped in again, the adjoint kernels run:
 //   adj_integrate   reverse of box collision and symplectic Euler (per particle)
 //   ADJ_FORCE pass  reverse of the symmetric pressure force (+boundary term),
 //                   the viscosity Laplacian and the clamped Tait EOS
@@ -146,13 +147,22 @@ inline u32 blocks(u32 n) { return (n + 255) / 256; }
 
 }  // namespace
 
+// The step buffers that the adjoint kernels read, for one step of a segment.
+struct StepSet {
+    DevBuf<float4> pos_b, vel_b, ap, vlap;
+    DevBuf<u32> perm, cstart, cend, mask;
+    DevBuf<u64> ckey, table;
+    DevBuf<float> rho, prs;
+    DevBuf<float2> dpr;
+};
+
 struct Adjoint {
     int steps = 0, every = 0;
     float dt = 0.f;
     bool have_forward = false;
     DevBuf<float4> ck_pos, ck_vel;   // [n_ckpt * n]
     DevBuf<u32> ck_ids;
-    DevBuf<float4> seg_pos, seg_vel; // [every * n] step inputs of one segment
+    std::vector<StepSet> seg;        // one buffer set per step of a segment
     DevBuf<u32> ids_a, ids_b;
     DevBuf<float4> target;
     DevBuf<float4> final_pos, final_vel;
@@ -179,7 +189,15 @@ float CUDASPHSimulator::rollout_forward(int steps, float dt, int every, const fl
     A.steps = steps; A.every = every; A.dt = dt;
     A.ck_pos.alloc(static_cast<size_t>(nck) * n); A.ck_vel.alloc(static_cast<size_t>(nck) * n);
     A.ck_ids.alloc(static_cast<size_t>(nck) * n);
-    A.seg_pos.alloc(static_cast<size_t>(every) * n); A.seg_vel.alloc(static_cast<size_t>(every) * n);
+    if (static_cast<int>(A.seg.size()) != every) A.seg = std::vector<StepSet>(every);
+    for (StepSet& b : A.seg) {
+        if (b.pos_b.count != n) {
+            b.pos_b.alloc(n); b.vel_b.alloc(n); b.ap.alloc(n); b.vlap.alloc(n);
+            b.perm.alloc(n); b.ckey.alloc(n); b.rho.alloc(n); b.prs.alloc(n); b.dpr.alloc(n);
+        }
+        if (b.table.count != table_size_) { b.table.alloc(table_size_); b.cstart.alloc(table_size_); b.cend.alloc(table_size_); }
+        if (b.mask.count != mask_.count) b.mask.alloc(mask_.count);
+    }
     A.ids_a.alloc(n); A.ids_b.alloc(n);
     A.target.alloc(n); A.final_pos.alloc(n); A.final_vel.alloc(n);
     A.xbar.alloc(n); A.vbar.alloc(n); A.xbar_s.alloc(n); A.vbar_s.alloc(n); A.abar.alloc(n); A.w.alloc(n);
@@ -222,6 +240,13 @@ void CUDASPHSimulator::rollout_backward(float* grad_v0, float* grad_visc, float*
     Adjoint& A = *static_cast<Adjoint*>(adjoint_);
     const u32 n = n_;
     const float dt = A.dt;
+    // exchanges the context's step buffers with a segment step's set (pointer swaps)
+    auto swap_step = [this](StepSet& b) {
+        std::swap(pos_b_, b.pos_b); std::swap(vel_b_, b.vel_b); std::swap(ap_, b.ap); std::swap(vlap_, b.vlap);
+        std::swap(perm_, b.perm); std::swap(cstart_, b.cstart); std::swap(cend_, b.cend); std::swap(mask_, b.mask);
+        std::swap(ckey_, b.ckey); std::swap(table_, b.table); std::swap(rho_, b.rho); std::swap(prs_, b.prs);
+        std::swap(dpr_, b.dpr);
+    };
     const float np_dt = dt < params_.non_pressure_max_time_step ? dt : params_.non_pressure_max_time_step;
     // dL/dx_T in the final state order, dL/dv_T = 0
     WCSPH_CUDA(cudaMemsetAsync(A.accum.ptr, 0, sizeof(double) * 3, stream_));
@@ -236,25 +261,14 @@ void CUDASPHSimulator::rollout_backward(float* grad_v0, float* grad_visc, float*
                                    cudaMemcpyDeviceToDevice, stream_));
         WCSPH_CUDA(cudaMemcpyAsync(vel_a_.ptr, A.ck_vel.ptr + static_cast<size_t>(seg) * n, sizeof(float4) * n,
                                    cudaMemcpyDeviceToDevice, stream_));
-        for (int s = s0; s < s1; ++s) {  // regenerate the step inputs of the segment
-            const size_t off = static_cast<size_t>(s - s0) * n;
-            WCSPH_CUDA(cudaMemcpyAsync(A.seg_pos.ptr + off, pos_a_.ptr, sizeof(float4) * n, cudaMemcpyDeviceToDevice,
-                                       stream_));
-            WCSPH_CUDA(cudaMemcpyAsync(A.seg_vel.ptr + off, vel_a_.ptr, sizeof(float4) * n, cudaMemcpyDeviceToDevice,
-                                       stream_));
-            if (s + 1 < s1) enqueue_fixed_step(dt);
+        for (int s = s0; s < s1; ++s) {  // re-run the segment, each step into its own buffer set
+            swap_step(A.seg[s - s0]);
+            enqueue_fixed_step(dt);
+            swap_step(A.seg[s - s0]);
         }
         for (int s = s1 - 1; s >= s0; --s) {
-            const size_t off = static_cast<size_t>(s - s0) * n;
-            WCSPH_CUDA(cudaMemcpyAsync(pos_a_.ptr, A.seg_pos.ptr + off, sizeof(float4) * n, cudaMemcpyDeviceToDevice,
-                                       stream_));
-            WCSPH_CUDA(cudaMemcpyAsync(vel_a_.ptr, A.seg_vel.ptr + off, sizeof(float4) * n, cudaMemcpyDeviceToDevice,
-                                       stream_));
-            // recompute the neighbourhood search, density and forces of step s
-            enqueue_search(true);
+            swap_step(A.seg[s - s0]);   // step s's sorted input, search and forces
             TravArgs a = fixed_args(dt);
-            launch_pass(PASS_DENSITY, dp_, a, stream_, cfg_.warps_density);
-            launch_pass(PASS_FORCE, dp_, a, stream_, cfg_.warps_force);
             adj_integrate_kernel<<<blocks(n), 256, 0, stream_>>>(dp_, pos_b_.ptr, vel_b_.ptr, ap_.ptr, vlap_.ptr,
                                                                  box_dev_.ptr, dt, np_dt, A.xbar.ptr, A.vbar.ptr,
                                                                  A.xbar_s.ptr, A.vbar_s.ptr, A.abar.ptr, A.w.ptr, n,
@@ -270,6 +284,7 @@ void CUDASPHSimulator::rollout_backward(float* grad_v0, float* grad_visc, float*
             unsort_kernel<<<blocks(n), 256, 0, stream_>>>(perm_.ptr, A.xbar_s.ptr, A.vbar_s.ptr, A.xbar.ptr,
                                                           A.vbar.ptr, n);
             WCSPH_CUDA(cudaGetLastError());
+            swap_step(A.seg[s - s0]);
         }
     }
     double acc[3];

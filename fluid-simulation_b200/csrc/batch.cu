@@ -108,6 +108,7 @@ struct BatchSim {
         a.boundary = HashView{btable.ptr, bcstart.ptr, bcend.ptr, btable_size ? btable_size - 1 : 0};
         a.mask = mask.ptr;
         a.mask_words = static_cast<u32>(mask_words);
+        a.chunk = n < (1u << 18) ? 8u : 32u;
         a.rho = rho.ptr; a.prs = prs.ptr; a.dpr = dpr.ptr;
         a.ap = ap.ptr; a.normal = normal.ptr; a.vlap = vlap.ptr; a.anp = anp.ptr;
         a.pos_out = pos_a.ptr; a.vel_out = vel_a.ptr;
@@ -246,7 +247,7 @@ static void build_batch(BatchSim& B, const wcsph_params& p, const wcsph_batch_sc
     B.table.alloc(B.table_size); B.cstart.alloc(B.table_size); B.cend.alloc(B.table_size);
     B.mask.alloc(n * static_cast<size_t>(B.mask_words));
     B.rho.alloc(n); B.prs.alloc(n); B.dpr.alloc(n); B.ap.alloc(n); B.normal.alloc(n); B.vlap.alloc(n); B.anp.alloc(n);
-    B.partials.alloc(2ull * (pass_grid(B.n, 2) + 1));
+    B.partials.alloc(2ull * (pass_grid(B.n, 2, 8) + 1));
     B.metric_sums.alloc(2ull * S);
     B.st.alloc(1);
     B.scenes.alloc(S);

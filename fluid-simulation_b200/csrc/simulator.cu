@@ -70,6 +70,11 @@ DevParams make_dev_params(const wcsph_params& p) {
     return d;
 }
 
+uint32_t effective_chunk(const StepConfig& c, uint32_t n) {
+    if (c.chunk == 8 || c.chunk == 16 || c.chunk == 32) return static_cast<uint32_t>(c.chunk);
+    return n < (1u << 18) ? 8u : 32u;
+}
+
 float metric_mass(const wcsph_params& p) {
     const float s = 2.f * p.particle_radius;
     const float volume = static_cast<float>(static_cast<double>(s * s * s) * 0.8);  // sph.cuh:20
@@ -151,7 +156,7 @@ void CUDASPHSimulator::allocate() {
     rho_.alloc(n); prs_.alloc(n); dpr_.alloc(n);
     ap_.alloc(n); normal_.alloc(n); vlap_.alloc(n); anp_.alloc(n);
     st_.alloc(1); box_dev_.alloc(1); metrics_dev_.alloc(2);
-    partials_.alloc(2ull * (pass_grid(n_, 2) + 1));
+    partials_.alloc(2ull * (pass_grid(n_, 2, 8) + 1));  // largest grid: 2 warps x 8 particles
     ensure_tables();
     WCSPH_CUDA(cudaMemsetAsync(hist_.ptr, 0, hist_.bytes(), stream_));
     WCSPH_CUDA(cudaMemsetAsync(st_.ptr, 0, sizeof(DevState), stream_));
@@ -252,6 +257,7 @@ TravArgs CUDASPHSimulator::trav_args(float delta) {
     a.boundary = HashView{btable_.ptr, bcstart_.ptr, bcend_.ptr, btable_size_ ? btable_size_ - 1 : 0};
     a.mask = mask_.ptr;
     a.mask_words = static_cast<u32>(cfg_.mask_words);
+    a.chunk = effective_chunk(cfg_, n_);
     a.rho = rho_.ptr; a.prs = prs_.ptr; a.dpr = dpr_.ptr;
     a.ap = ap_.ptr; a.normal = normal_.ptr; a.vlap = vlap_.ptr; a.anp = anp_.ptr;
     a.pos_out = pos_a_.ptr; a.vel_out = vel_a_.ptr;
@@ -408,6 +414,8 @@ void CUDASPHSimulator::set_params(const wcsph_params& p) {
 void CUDASPHSimulator::apply_config(const StepConfig& c) {
     if (c == cfg_) return;
     if (c.mask_words < 1 || c.mask_words > 16) throw Error(WCSPH_ERR_CONFIG, "mask_words must be in [1, 16]");
+    if (c.chunk != 0 && c.chunk != 8 && c.chunk != 16 && c.chunk != 32)
+        throw Error(WCSPH_ERR_CONFIG, "particles_per_warp must be 8, 16 or 32");
     cfg_ = c;
     params_.cell_size_mult = c.cell_size_mult;
     params_.table_size_mult = c.table_size_mult;

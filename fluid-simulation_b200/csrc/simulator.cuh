@@ -75,10 +75,15 @@ struct StepConfig {
     int warps_force = 2;
     int warps_surface = 2;
     int mask_words = 10;        // neighbour bit-matrix words per particle (cap = 32*words)
+    int chunk = 0;              // sorted particles per warp: 8, 16, 32; 0 = by scene size
     float cell_size_mult = 1.f;
     uint32_t table_size_mult = 1;
     bool operator==(const StepConfig&) const = default;
 };
+// Particles per warp chunk of the traversal passes: the configured value, or
+// 8 below 2^18 particles (more warps for small scenes) and 32 above.
+uint32_t effective_chunk(const StepConfig& c, uint32_t n);
+
 
 class FluidSimulator {
 public:

@@ -707,7 +707,8 @@ __global__ void __launch_bounds__(WPB * 32, 24 / WPB) cell_pass_kernel(const Dev
     float red_max = 0.f, red_speed = 0.f, red_speed2 = 0.f;
 
     const u32 chunk = blockIdx.x * WPB + warp;
-    const u32 base = chunk * 32u;
+    const u32 per_chunk = a.chunk;
+    const u32 base = chunk * per_chunk;
     const u32 n = a.n;
     const int R = a.range;
     const u32 D = static_cast<u32>(2 * R + 1);
@@ -716,10 +717,12 @@ __global__ void __launch_bounds__(WPB * 32, 24 / WPB) cell_pass_kernel(const Dev
 
     if (base < n) {
         const u32 i0l = base + lane;
-        const u64 my_pk = i0l < n ? a.ckey[i0l] : 0ull;
+        const bool in = lane < per_chunk && i0l < n;
+        const u64 my_pk = in ? a.ckey[i0l] : 0ull;
         u64 prev_pk = __shfl_up_sync(FULL, my_pk, 1);
         if (lane == 0) prev_pk = i0l > 0 ? a.ckey[i0l - 1] : ~my_pk;
-        u32 starts = __ballot_sync(FULL, i0l < n && (i0l == 0 || my_pk != prev_pk));
+        // cells that start in this chunk (a cell is handled whole by the warp of its first particle)
+        u32 starts = __ballot_sync(FULL, in && (i0l == 0 || my_pk != prev_pk));
         while (starts) {
             const u32 s = __ffs(starts) - 1;
             starts &= starts - 1;
@@ -1159,8 +1162,8 @@ __global__ void boundary_mass_kernel(const DevParams P, const float4* __restrict
 
 }  // namespace
 
-u32 pass_grid(u32 n, int wpb) {
-    const u32 chunks = (n + 31) / 32;
+u32 pass_grid(u32 n, int wpb, u32 chunk) {
+    const u32 chunks = (n + chunk - 1) / chunk;
     return (chunks + wpb - 1) / wpb;
 }
 
@@ -1196,7 +1199,7 @@ static void launch_wpb(const DevParams& P, const TravArgs& a, cudaStream_t strea
 
 template <int KIND, bool BATCH>
 static void launch_kind(const DevParams& P, const TravArgs& a, cudaStream_t stream, int wpb) {
-    const u32 grid = pass_grid(a.n, wpb);
+    const u32 grid = pass_grid(a.n, wpb, a.chunk);
     if (grid == 0) return;
     switch (wpb) {
     case 2: launch_wpb<KIND, 2, BATCH>(P, a, stream, grid); break;

@@ -14,8 +14,9 @@
 //                   CFL max |v|^2 and metric reductions
 //                   (compute_non_pressure_accel.cu + update_positions.cu:14-68)
 //
-// Work decomposition (all passes): one warp per 32-particle chunk of the
-// sorted array; for every cell that starts inside the chunk, the warp looks
+// Work decomposition (all passes): one warp per chunk of 8, 16 or 32
+// particles of the sorted array (small scenes use small chunks so that more
+// warps run); for every cell that starts inside the chunk, the warp looks
 // up the (2R+1)^3 neighbour cells once (lane-parallel hash probes) and
 // stages their particles (the candidates, in the reference's cell order)
 // into shared memory. The home particles are taken in blocks of up to 32.
@@ -60,6 +61,7 @@ struct TravArgs {
     // neighbour bitmasks
     u32* mask;
     u32 mask_words;           // words per particle (candidate cap = 32*mask_words)
+    u32 chunk;                // sorted particles per warp chunk: 8, 16 or 32
     // fields
     float* rho;
     float* prs;
@@ -108,7 +110,8 @@ void launch_reorder_cells(const float4* pos_in, const float4* vel_in, const u32*
 
 void launch_pass(int kind, const DevParams& P, const TravArgs& a, cudaStream_t stream, int warps_per_block,
                  bool batch = false);
-u32 pass_grid(u32 n, int warps_per_block);
+// Blocks of a traversal pass over n particles (chunk particles per warp).
+u32 pass_grid(u32 n, int warps_per_block, u32 chunk);
 
 // CFL max |v|^2 of a velocity array into st->vmax2_bits[st->parity].
 void launch_init_cfl(const float4* vel, u32 n, DevState* st, cudaStream_t stream);

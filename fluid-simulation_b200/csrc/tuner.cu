@@ -12,6 +12,7 @@ namespace wcsph {
 namespace {
 const int kWarps[] = {2, 4, 8};
 const int kMaskWords[] = {8, 10, 12, 16};
+const int kChunk[] = {8, 16, 32};
 const double kCellMult[] = {0.5, 2. / 3., 1., 1.5, 2.};  // step_tuner.cuh:88
 const uint32_t kTableMult[] = {1, 2, 4, 8, 16, 32};      // step_tuner.cuh:251-256
 
@@ -135,13 +136,15 @@ Tuner::Tuner(CUDASPHSimulator* sim) : sim_(sim) {
         for (int wf : kWarps)
             for (int ws : kWarps)
                 for (int mw : kMaskWords)
-                    for (double cm : kCellMult)
-                        for (uint32_t tm : kTableMult) {
-                            StepConfig c;
-                            c.warps_density = wd; c.warps_force = wf; c.warps_surface = ws;
-                            c.mask_words = mw; c.cell_size_mult = static_cast<float>(cm); c.table_size_mult = tm;
-                            if (config_allowed(c)) space_.push_back(c);
-                        }
+                    for (int ch : kChunk)
+                        for (double cm : kCellMult)
+                            for (uint32_t tm : kTableMult) {
+                                StepConfig c;
+                                c.warps_density = wd; c.warps_force = wf; c.warps_surface = ws;
+                                c.mask_words = mw; c.chunk = ch;
+                                c.cell_size_mult = static_cast<float>(cm); c.table_size_mult = tm;
+                                if (config_allowed(c)) space_.push_back(c);
+                            }
     visited_.assign(space_.size(), 0);
     best_cfg_ = sim->config();
 }
@@ -205,7 +208,7 @@ int Tuner::next_candidate() {
     const StepConfig& cur = space_[current_];
     for (int attempt = 0; attempt < 64; ++attempt) {
         StepConfig c = cur;
-        std::uniform_int_distribution<int> which(0, 5), dir(0, 1);
+        std::uniform_int_distribution<int> which(0, 6), dir(0, 1);
         const int p = which(rng_);
         const int step = dir(rng_) ? 1 : -1;
         auto shift = [&](auto& field, const auto* values, int count) {
@@ -220,6 +223,7 @@ int Tuner::next_candidate() {
         case 1: shift(c.warps_force, kWarps, 3); break;
         case 2: shift(c.warps_surface, kWarps, 3); break;
         case 3: shift(c.mask_words, kMaskWords, 4); break;
+        case 6: shift(c.chunk, kChunk, 3); break;
         case 4: {
             int idx = 0;
             for (int k = 0; k < 5; ++k) if (static_cast<float>(kCellMult[k]) == c.cell_size_mult) idx = k;
@@ -269,6 +273,7 @@ StepConfig Tuner::parse_config_json(const std::string& text, const StepConfig& b
         else if (e.name == "compute_pressure_accel_n_normal_block") c.warps_force = warps_from_block(v);
         else if (e.name == "compute_non_pressure_accel_block") c.warps_surface = warps_from_block(v);
         else if (e.name == "mask_words") c.mask_words = static_cast<int>(v);
+        else if (e.name == "particles_per_warp") c.chunk = static_cast<int>(v);
         // KTT-only parameters (KERNEL_DIR, *_u_n, *_nlist, *_shared, *_cache_log2,
         // MIN_TABLE_SIZE, EXTERNAL_FORCE ...) have no counterpart and are ignored.
     }
@@ -277,6 +282,8 @@ StepConfig Tuner::parse_config_json(const std::string& text, const StepConfig& b
     if (c.table_size_mult == 0 || (c.table_size_mult & (c.table_size_mult - 1)) || c.table_size_mult > 64)
         throw Error(WCSPH_ERR_CONFIG, "TABLE_SIZE_MULT must be a power of two <= 64");
     if (c.mask_words < 1 || c.mask_words > 16) throw Error(WCSPH_ERR_CONFIG, "mask_words must be in [1, 16]");
+    if (c.chunk != 0 && c.chunk != 8 && c.chunk != 16 && c.chunk != 32)
+        throw Error(WCSPH_ERR_CONFIG, "particles_per_warp must be 8, 16 or 32");
     return c;
 }
 
@@ -289,10 +296,11 @@ std::string Tuner::config_json(const StepConfig& c) {
                   "  {\"Name\": \"compute_rho_p_block\", \"Value\": %d, \"ValueType\": \"UnsignedInt\"},\n"
                   "  {\"Name\": \"compute_pressure_accel_n_normal_block\", \"Value\": %d, \"ValueType\": \"UnsignedInt\"},\n"
                   "  {\"Name\": \"compute_non_pressure_accel_block\", \"Value\": %d, \"ValueType\": \"UnsignedInt\"},\n"
-                  "  {\"Name\": \"mask_words\", \"Value\": %d, \"ValueType\": \"UnsignedInt\"}\n"
+                  "  {\"Name\": \"mask_words\", \"Value\": %d, \"ValueType\": \"UnsignedInt\"},\n"
+                  "  {\"Name\": \"particles_per_warp\", \"Value\": %d, \"ValueType\": \"UnsignedInt\"}\n"
                   "]\n",
                   static_cast<double>(c.cell_size_mult), c.table_size_mult, c.warps_density * 32,
-                  c.warps_force * 32, c.warps_surface * 32, c.mask_words);
+                  c.warps_force * 32, c.warps_surface * 32, c.mask_words, c.chunk);
     return buf;
 }
 
