@@ -71,6 +71,8 @@ struct BatchSim {
     DevBuf<u32> cstart, cend, mask;
     u32 table_size = 0;
     DevBuf<float> rho, prs, partials, metric_sums;
+    DevBuf<u32> group_done;
+    DevBuf<double> group_partials;
     DevBuf<float2> dpr;
     DevBuf<float4> ap, normal, vlap, anp;
     DevBuf<DevState> st;
@@ -123,6 +125,8 @@ struct BatchSim {
         a.np_max_dt = params.non_pressure_max_time_step;
         a.metric_mass = metric_mass;
         a.block_partials = partials.ptr;
+        a.group_done = group_done.ptr;
+        a.group_partials = group_partials.ptr;
         return a;
     }
 
@@ -247,7 +251,10 @@ static void build_batch(BatchSim& B, const wcsph_params& p, const wcsph_batch_sc
     B.table.alloc(B.table_size); B.cstart.alloc(B.table_size); B.cend.alloc(B.table_size);
     B.mask.alloc(n * static_cast<size_t>(B.mask_words));
     B.rho.alloc(n); B.prs.alloc(n); B.dpr.alloc(n); B.ap.alloc(n); B.normal.alloc(n); B.vlap.alloc(n); B.anp.alloc(n);
-    B.partials.alloc(2ull * (pass_grid(B.n, 2, 8) + 1));
+    B.partials.alloc(2ull * pass_max_warps(B.n));
+    B.group_done.alloc(pass_max_warps(B.n) / 32u + 1u);
+    B.group_partials.alloc(2ull * (pass_max_warps(B.n) / 32u + 1u));
+    WCSPH_CUDA(cudaMemsetAsync(B.group_done.ptr, 0, B.group_done.bytes(), B.stream));
     B.metric_sums.alloc(2ull * S);
     B.st.alloc(1);
     B.scenes.alloc(S);

@@ -156,7 +156,10 @@ void CUDASPHSimulator::allocate() {
     rho_.alloc(n); prs_.alloc(n); dpr_.alloc(n);
     ap_.alloc(n); normal_.alloc(n); vlap_.alloc(n); anp_.alloc(n);
     st_.alloc(1); box_dev_.alloc(1); metrics_dev_.alloc(2);
-    partials_.alloc(2ull * (pass_grid(n_, 2, 8) + 1));  // largest grid: 2 warps x 8 particles
+    partials_.alloc(2ull * pass_max_warps(n_));
+    group_done_.alloc(pass_max_warps(n_) / 32u + 1u);
+    group_partials_.alloc(2ull * (pass_max_warps(n_) / 32u + 1u));
+    WCSPH_CUDA(cudaMemsetAsync(group_done_.ptr, 0, group_done_.bytes(), stream_));
     ensure_tables();
     WCSPH_CUDA(cudaMemsetAsync(hist_.ptr, 0, hist_.bytes(), stream_));
     WCSPH_CUDA(cudaMemsetAsync(st_.ptr, 0, sizeof(DevState), stream_));
@@ -270,6 +273,8 @@ TravArgs CUDASPHSimulator::trav_args(float delta) {
     a.np_max_dt = params_.non_pressure_max_time_step;
     a.metric_mass = metric_mass_;
     a.block_partials = partials_.ptr;
+    a.group_done = group_done_.ptr;
+    a.group_partials = group_partials_.ptr;
     return a;
 }
 

@@ -72,7 +72,7 @@ float metric_mass(const wcsph_params& p);
 // Tunable launch configuration of the step (the autotuner's search space).
 struct StepConfig {
     int warps_density = 2;
-    int warps_force = 2;
+    int warps_force = 4;
     int warps_surface = 2;
     int mask_words = 10;        // neighbour bit-matrix words per particle (cap = 32*words)
     int chunk = 0;              // sorted particles per warp: 8, 16, 32; 0 = by scene size
@@ -190,6 +190,8 @@ private:
     DevBuf<float2> dpr_;
     DevBuf<float4> ap_, normal_, vlap_, anp_;
     DevBuf<float> partials_;
+    DevBuf<u32> group_done_;
+    DevBuf<double> group_partials_;
     DevBuf<DevState> st_;
     DevBuf<DevBox> box_dev_;
     DevBuf<float> metrics_dev_;

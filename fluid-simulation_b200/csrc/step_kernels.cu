@@ -46,6 +46,11 @@ struct KindCfg {
     static constexpr int nf = (KIND == PASS_FORCE || KIND == PASS_ADJ_FORCE) ? 9
                               : (KIND == PASS_SURFACE || KIND == PASS_ADJ_DENSITY) ? 3 : 1;
     static constexpr int nfb = KIND == PASS_ADJ_FORCE ? 4 : (KIND == PASS_DENSITY ? 1 : 3);
+    // resident warps per SM the register allocation must allow (32 -> 64 registers,
+    // 24 -> 80, 16 -> 128): the force pass spills below 80 registers, the
+    // adjoint force pass below 128
+    static constexpr int min_warps =
+        (KIND == PASS_DENSITY || KIND == PASS_SURFACE) ? 32 : (KIND == PASS_ADJ_FORCE ? 16 : 24);
 };
 
 __host__ __device__ constexpr size_t align16(size_t b) { return (b + 15) & ~static_cast<size_t>(15); }
@@ -65,7 +70,7 @@ struct WarpView {
     u32* bstart;
     u32* bpref;
     float* part;   // [SEG_SLOTS][nf] segment partials
-    u32* aux;      // density: the block's bit matrix (cap words); others: row hit offsets
+    u32* aux;      // the block's bit matrix (cap words)
     u32* hoff;     // row hit offsets (HOME_BLOCK + 1)
 };
 
@@ -91,7 +96,8 @@ __host__ __device__ __forceinline__ size_t warp_smem_bytes(u32 cap, WarpView<KIN
         bpref = take(4ull * (MAX_BOUNDARY_CELLS + 3));
     }
     unsigned char* part = take(4ull * SEG_SLOTS * C::nf);
-    unsigned char* aux = KIND == PASS_DENSITY ? take(4ull * cap) : nullptr;
+    // the block's bit matrix (density builds it here; the later passes copy it in)
+    unsigned char* aux = (KIND == PASS_COUNT || KIND == PASS_FILL) ? nullptr : take(4ull * cap);
     unsigned char* hoff = take(4ull * (HOME_BLOCK + 4));
     if (v) {
         v->sa = reinterpret_cast<float4*>(sa);
@@ -679,14 +685,11 @@ __device__ __forceinline__ u32 boundary_pair_run(const WarpView<KIND>& S, const 
 }
 
 template <int KIND, int WPB, bool BATCH>
-__global__ void __launch_bounds__(WPB * 32, 24 / WPB) cell_pass_kernel(const DevParams P, const TravArgs a) {
+__global__ void __launch_bounds__(WPB * 32, KindCfg<KIND>::min_warps / WPB) cell_pass_kernel(const DevParams P, const TravArgs a) {
     using C = KindCfg<KIND>;
     constexpr int NF = C::nf;
     constexpr int NFB = C::nfb;
     extern __shared__ __align__(16) unsigned char dyn_smem[];
-    __shared__ float s_dt, s_np_dt;
-    __shared__ float s_red[WPB][3];
-    __shared__ bool s_last;
     const u32 lane = lane_id();
     const u32 warp = threadIdx.x >> 5;
     const u32 cap = a.mask_words * 32u;
@@ -696,13 +699,12 @@ __global__ void __launch_bounds__(WPB * 32, 24 / WPB) cell_pass_kernel(const Dev
 
     float dt = 0.f, np_dt = 0.f;
     if constexpr (KIND == PASS_SURFACE) {
-        if (threadIdx.x == 0) {
-            s_dt = cfl_time_step(a, P);
-            s_np_dt = a.delta < a.np_max_dt ? a.delta : a.np_max_dt;
-        }
-        __syncthreads();
-        dt = s_dt;
-        np_dt = s_np_dt;
+        // every warp reads the CFL step itself (no block barrier); the flip of
+        // the max-speed parity happens only after every warp has finished
+        float t = 0.f;
+        if (lane == 0) t = cfl_time_step(a, P);
+        dt = __shfl_sync(FULL, t, 0);
+        np_dt = a.delta < a.np_max_dt ? a.delta : a.np_max_dt;
     }
     float red_max = 0.f, red_speed = 0.f, red_speed2 = 0.f;
 
@@ -883,8 +885,12 @@ __global__ void __launch_bounds__(WPB * 32, 24 / WPB) cell_pass_kernel(const Dev
                     }
                 } else {
                     if (masked) {
+                        // one coalesced copy of the block's bit matrix, then walks in shared memory
+                        const u32 nwords = (nh * Mrow) >> 5;
+                        for (u32 w = lane; w < nwords; w += 32) S.aux[w] = __ldg(blk_bits + w);
+                        __syncwarp();
                         u32 lo, hi;
-                        const u32 c = fluid_hit_run<KIND>(S, P, a, blk_bits, nh, Mrow, i0, lo, hi);
+                        const u32 c = fluid_hit_run<KIND, true>(S, P, a, S.aux, nh, Mrow, i0, lo, hi);
                         if (c) combine<NF>(S.part, res, act, lo, hi, c);
                     } else {
                         for (u32 c0 = 0; c0 < M; c0 += cap) {
@@ -993,51 +999,66 @@ __global__ void __launch_bounds__(WPB * 32, 24 / WPB) cell_pass_kernel(const Dev
         if (lane == 0 && v != 0.0) atomicAdd(a.adj_accum, v);
     }
     if constexpr (KIND == PASS_SURFACE) {
-        // block reduction -> per-block partials (deterministic final sum)
+        // CFL max |v|^2 and the metric sums without block barriers: warp
+        // partials -> groups of 32 warps -> whole grid; each level is finished
+        // by its last arriving warp and summed in index order (deterministic).
         for (int o = 16; o > 0; o >>= 1) {
             red_max = fmaxf(red_max, __shfl_xor_sync(FULL, red_max, o));
             red_speed += __shfl_xor_sync(FULL, red_speed, o);
             red_speed2 += __shfl_xor_sync(FULL, red_speed2, o);
         }
-        if (lane == 0) { s_red[warp][0] = red_max; s_red[warp][1] = red_speed; s_red[warp][2] = red_speed2; }
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            float m = 0.f, s1 = 0.f, s2 = 0.f;
-            for (int w = 0; w < WPB; ++w) { m = fmaxf(m, s_red[w][0]); s1 += s_red[w][1]; s2 += s_red[w][2]; }
-            a.block_partials[2 * blockIdx.x] = s1;
-            a.block_partials[2 * blockIdx.x + 1] = s2;
-            atomicMax(&a.st->vmax2_bits[a.st->parity ^ 1u], __float_as_uint(m));
+        const u32 nwarps = gridDim.x * WPB;
+        const u32 gw = blockIdx.x * WPB + warp;
+        const u32 group = gw >> 5;
+        const u32 ngroups = (nwarps + 31u) >> 5;
+        const u32 gsize = min(32u, nwarps - (group << 5));
+        u32 last = 0;
+        if (lane == 0) {
+            a.block_partials[2 * gw] = red_speed;
+            a.block_partials[2 * gw + 1] = red_speed2;
+            atomicMax(&a.st->vmax2_bits[a.st->parity ^ 1u], __float_as_uint(red_max));
             __threadfence();
-            const u32 prev = atomicAdd(&a.st->blocks_done, 1u);
-            s_last = (prev == gridDim.x - 1);
+            last = atomicAdd(a.group_done + group, 1u) == gsize - 1 ? 1u : 0u;
         }
-        __syncthreads();
-        if (s_last) {
+        if (__shfl_sync(FULL, last, 0)) {
             __threadfence();
-            double s1 = 0.0, s2 = 0.0;
-            for (u32 b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
-                s1 += static_cast<double>(__ldcg(a.block_partials + 2 * b));
-                s2 += static_cast<double>(__ldcg(a.block_partials + 2 * b + 1));
-            }
+            const u32 w = (group << 5) + lane;
+            double s1 = lane < gsize ? static_cast<double>(__ldcg(a.block_partials + 2 * w)) : 0.0;
+            double s2 = lane < gsize ? static_cast<double>(__ldcg(a.block_partials + 2 * w + 1)) : 0.0;
             for (int o = 16; o > 0; o >>= 1) {
                 s1 += __shfl_xor_sync(FULL, s1, o);
                 s2 += __shfl_xor_sync(FULL, s2, o);
             }
-            __shared__ double s_d[WPB][2];
-            if (lane == 0) { s_d[warp][0] = s1; s_d[warp][1] = s2; }
-            __syncthreads();
-            if (threadIdx.x == 0) {
+            u32 top = 0;
+            if (lane == 0) {
+                a.group_partials[2 * group] = s1;
+                a.group_partials[2 * group + 1] = s2;
+                a.group_done[group] = 0u;
+                __threadfence();
+                top = atomicAdd(&a.st->blocks_done, 1u) == ngroups - 1 ? 1u : 0u;
+            }
+            if (__shfl_sync(FULL, top, 0)) {
+                __threadfence();
                 double t1 = 0.0, t2 = 0.0;
-                for (int w = 0; w < WPB; ++w) { t1 += s_d[w][0]; t2 += s_d[w][1]; }
-                DevState* st = a.st;
-                st->last_mean_speed = static_cast<float>(t1 / static_cast<double>(n));
-                st->last_ke = static_cast<float>(0.5 * static_cast<double>(a.metric_mass) * t2);
-                st->last_dt_p = dt;
-                st->last_np_dt = np_dt;
-                const u32 old = st->parity;
-                st->vmax2_bits[old] = 0u;
-                st->parity = old ^ 1u;
-                st->blocks_done = 0u;
+                for (u32 g = lane; g < ngroups; g += 32) {
+                    t1 += __ldcg(a.group_partials + 2 * g);
+                    t2 += __ldcg(a.group_partials + 2 * g + 1);
+                }
+                for (int o = 16; o > 0; o >>= 1) {
+                    t1 += __shfl_xor_sync(FULL, t1, o);
+                    t2 += __shfl_xor_sync(FULL, t2, o);
+                }
+                if (lane == 0) {
+                    DevState* st = a.st;
+                    st->last_mean_speed = static_cast<float>(t1 / static_cast<double>(n));
+                    st->last_ke = static_cast<float>(0.5 * static_cast<double>(a.metric_mass) * t2);
+                    st->last_dt_p = dt;
+                    st->last_np_dt = np_dt;
+                    const u32 old = st->parity;
+                    st->vmax2_bits[old] = 0u;
+                    st->parity = old ^ 1u;
+                    st->blocks_done = 0u;
+                }
             }
         }
     }

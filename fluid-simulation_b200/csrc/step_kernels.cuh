@@ -81,7 +81,9 @@ struct TravArgs {
     float cfl_factor;
     float max_dt, min_dt, np_max_dt;
     float metric_mass;        // host-side PARTICLE_MASS used by the ke metric
-    float* block_partials;    // [gridDim.x][2] sum|v|, sum|v|^2
+    float* block_partials;    // [warps][2] sum|v|, sum|v|^2 per warp of the surface pass
+    u32* group_done;          // [ceil(warps / 32)] arrival counters (zero between launches)
+    double* group_partials;   // [ceil(warps / 32)][2]
     // adjoint passes (differentiable rollout)
     const float4* adj_abar;   // dL/da_p per sorted particle
     const float4* adj_w;      // dL/d(vlap) = nu*10*m * dL/da_np
@@ -112,6 +114,9 @@ void launch_pass(int kind, const DevParams& P, const TravArgs& a, cudaStream_t s
                  bool batch = false);
 // Blocks of a traversal pass over n particles (chunk particles per warp).
 u32 pass_grid(u32 n, int warps_per_block, u32 chunk);
+// Upper bound of the warps of any traversal launch over n particles (chunk >= 8,
+// at most 8 warps per block): sizes the surface pass's reduction buffers.
+inline u32 pass_max_warps(u32 n) { return (n + 7u) / 8u + 8u; }
 
 // CFL max |v|^2 of a velocity array into st->vmax2_bits[st->parity].
 void launch_init_cfl(const float4* vel, u32 n, DevState* st, cudaStream_t stream);
