@@ -153,7 +153,6 @@ struct StepSet {
     DevBuf<u32> perm, cstart, cend, mask;
     DevBuf<u64> ckey, table;
     DevBuf<float> rho, prs;
-    DevBuf<float2> dpr;
 };
 
 struct Adjoint {
@@ -193,7 +192,7 @@ float CUDASPHSimulator::rollout_forward(int steps, float dt, int every, const fl
     for (StepSet& b : A.seg) {
         if (b.pos_b.count != n) {
             b.pos_b.alloc(n); b.vel_b.alloc(n); b.ap.alloc(n); b.vlap.alloc(n);
-            b.perm.alloc(n); b.ckey.alloc(n); b.rho.alloc(n); b.prs.alloc(n); b.dpr.alloc(n);
+            b.perm.alloc(n); b.ckey.alloc(n); b.rho.alloc(n); b.prs.alloc(n);
         }
         if (b.table.count != table_size_) { b.table.alloc(table_size_); b.cstart.alloc(table_size_); b.cend.alloc(table_size_); }
         if (b.mask.count != mask_.count) b.mask.alloc(mask_.count);
@@ -245,7 +244,6 @@ void CUDASPHSimulator::rollout_backward(float* grad_v0, float* grad_visc, float*
         std::swap(pos_b_, b.pos_b); std::swap(vel_b_, b.vel_b); std::swap(ap_, b.ap); std::swap(vlap_, b.vlap);
         std::swap(perm_, b.perm); std::swap(cstart_, b.cstart); std::swap(cend_, b.cend); std::swap(mask_, b.mask);
         std::swap(ckey_, b.ckey); std::swap(table_, b.table); std::swap(rho_, b.rho); std::swap(prs_, b.prs);
-        std::swap(dpr_, b.dpr);
     };
     const float np_dt = dt < params_.non_pressure_max_time_step ? dt : params_.non_pressure_max_time_step;
     // dL/dx_T in the final state order, dL/dv_T = 0

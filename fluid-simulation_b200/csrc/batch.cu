@@ -73,7 +73,7 @@ struct BatchSim {
     DevBuf<float> rho, prs, partials, metric_sums;
     DevBuf<u32> group_done;
     DevBuf<double> group_partials;
-    DevBuf<float2> dpr;
+    DevBuf<float4> xq, vq, xr;
     DevBuf<float4> ap, normal, vlap, anp;
     DevBuf<DevState> st;
     DevBuf<DevScene> scenes;
@@ -111,7 +111,8 @@ struct BatchSim {
         a.mask = mask.ptr;
         a.mask_words = static_cast<u32>(mask_words);
         a.chunk = n < (1u << 18) ? 8u : 32u;
-        a.rho = rho.ptr; a.prs = prs.ptr; a.dpr = dpr.ptr;
+        a.rho = rho.ptr; a.prs = prs.ptr;
+        a.xq = xq.ptr; a.vq = vq.ptr; a.xr = xr.ptr;
         a.ap = ap.ptr; a.normal = normal.ptr; a.vlap = vlap.ptr; a.anp = anp.ptr;
         a.pos_out = pos_a.ptr; a.vel_out = vel_a.ptr;
         a.box = nullptr;
@@ -250,7 +251,7 @@ static void build_batch(BatchSim& B, const wcsph_params& p, const wcsph_batch_sc
     B.table_size = static_cast<u32>(std::max<u64>(std::bit_ceil(static_cast<u64>(n)) / 4, 64) * p.table_size_mult);
     B.table.alloc(B.table_size); B.cstart.alloc(B.table_size); B.cend.alloc(B.table_size);
     B.mask.alloc(n * static_cast<size_t>(B.mask_words));
-    B.rho.alloc(n); B.prs.alloc(n); B.dpr.alloc(n); B.ap.alloc(n); B.normal.alloc(n); B.vlap.alloc(n); B.anp.alloc(n);
+    B.rho.alloc(n); B.prs.alloc(n); B.xq.alloc(n); B.vq.alloc(n); B.xr.alloc(n); B.ap.alloc(n); B.normal.alloc(n); B.vlap.alloc(n); B.anp.alloc(n);
     B.partials.alloc(2ull * pass_max_warps(B.n));
     B.group_done.alloc(pass_max_warps(B.n) / 32u + 1u);
     B.group_partials.alloc(2ull * (pass_max_warps(B.n) / 32u + 1u));

@@ -153,7 +153,7 @@ void CUDASPHSimulator::allocate() {
     offsets_.alloc(SORT_DIGITS * 256);
     lookback_.alloc(static_cast<size_t>(SORT_DIGITS) * sort_tiles(n_) * 256);
     perm_.alloc(n); ckey_.alloc(n);
-    rho_.alloc(n); prs_.alloc(n); dpr_.alloc(n);
+    rho_.alloc(n); prs_.alloc(n); xq_.alloc(n); vq_.alloc(n); xr_.alloc(n);
     ap_.alloc(n); normal_.alloc(n); vlap_.alloc(n); anp_.alloc(n);
     st_.alloc(1); box_dev_.alloc(1); metrics_dev_.alloc(2);
     partials_.alloc(2ull * pass_max_warps(n_));
@@ -261,7 +261,8 @@ TravArgs CUDASPHSimulator::trav_args(float delta) {
     a.mask = mask_.ptr;
     a.mask_words = static_cast<u32>(cfg_.mask_words);
     a.chunk = effective_chunk(cfg_, n_);
-    a.rho = rho_.ptr; a.prs = prs_.ptr; a.dpr = dpr_.ptr;
+    a.rho = rho_.ptr; a.prs = prs_.ptr;
+    a.xq = xq_.ptr; a.vq = vq_.ptr; a.xr = xr_.ptr;
     a.ap = ap_.ptr; a.normal = normal_.ptr; a.vlap = vlap_.ptr; a.anp = anp_.ptr;
     a.pos_out = pos_a_.ptr; a.vel_out = vel_a_.ptr;
     a.box = box_dev_.ptr;

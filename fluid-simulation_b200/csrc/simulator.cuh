@@ -187,7 +187,7 @@ private:
     uint32_t table_size_ = 0;
     DevBuf<u32> mask_;
     DevBuf<float> rho_, prs_;
-    DevBuf<float2> dpr_;
+    DevBuf<float4> xq_, vq_, xr_;
     DevBuf<float4> ap_, normal_, vlap_, anp_;
     DevBuf<float> partials_;
     DevBuf<u32> group_done_;

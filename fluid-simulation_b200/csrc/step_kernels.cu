@@ -211,6 +211,7 @@ __device__ __forceinline__ void stage(const WarpView<KIND>& S, const TravArgs& a
 // A neighbour's data as the pair arithmetic reads it.
 //   x: position; FORCE: b = (v_j, 1 / rho_j), c = p_j / rho_j^2;
 //   SURFACE: b = n_j, c = rho_j; j: particle index (passes that address j).
+// Force and surface read two 16-byte records per neighbour (xq, vq / xr, normal).
 struct Nbr {
     float4 x, b;
     float c;
@@ -225,16 +226,14 @@ __device__ __forceinline__ Nbr fetch(const WarpView<KIND>& S, const TravArgs& a,
         d.x = make_float4(f[0], f[2], f[4], 0.f);
     } else if constexpr (KIND == PASS_FORCE) {
         d.j = S.cand[m];
-        d.x = __ldg(a.pos + d.j);
-        d.b = __ldg(a.vel + d.j);
-        const float2 q = __ldg(a.dpr + d.j);
-        d.b.w = q.y;
-        d.c = q.x;
+        d.x = __ldg(a.xq + d.j);
+        d.b = __ldg(a.vq + d.j);
+        d.c = d.x.w;
     } else if constexpr (KIND == PASS_SURFACE) {
         d.j = S.cand[m];
-        d.x = __ldg(a.pos + d.j);
+        d.x = __ldg(a.xr + d.j);
         d.b = __ldg(a.normal + d.j);
-        d.c = __ldg(a.rho + d.j);
+        d.c = d.x.w;
     } else {
         d.j = S.cand[m];
         d.x = S.sa[m];
@@ -282,11 +281,16 @@ struct HomeData {
 template <int KIND>
 __device__ __forceinline__ HomeData load_home(const TravArgs& a, u32 i) {
     HomeData H;
-    H.x = __ldg(a.pos + i);
     if constexpr (KIND == PASS_FORCE) {
-        H.v = __ldg(a.vel + i);
+        H.x = __ldg(a.xq + i);   // w = p / rho^2
+        H.v = __ldg(a.vq + i);
         H.prs = __ldg(a.prs + i);
-        H.dpi = __ldg(a.dpr + i).x;
+        H.dpi = H.x.w;
+    } else if constexpr (KIND == PASS_SURFACE) {
+        H.x = __ldg(a.xr + i);   // w = rho
+        H.rho = H.x.w;
+    } else {
+        H.x = __ldg(a.pos + i);
     }
     if constexpr (KIND == PASS_ADJ_FORCE) {
         H.v = __ldg(a.vel + i);
@@ -294,10 +298,7 @@ __device__ __forceinline__ HomeData load_home(const TravArgs& a, u32 i) {
         H.prs = __ldg(a.prs + i);
         H.dpi = H.prs / (H.rho * H.rho);
     }
-    if constexpr (KIND == PASS_SURFACE) {
-        H.rho = __ldg(a.rho + i);
-        H.n = __ldg(a.normal + i);
-    }
+    if constexpr (KIND == PASS_SURFACE) H.n = __ldg(a.normal + i);
     if constexpr (KIND == PASS_ADJ_FORCE) {
         H.abar = __ldg(a.adj_abar + i);
         H.w = __ldg(a.adj_w + i);
@@ -919,8 +920,11 @@ __global__ void __launch_bounds__(WPB * 32, KindCfg<KIND>::min_warps / WPB) cell
                         const float prs = tait_pressure(rho, P);
                         a.rho[i] = rho;
                         a.prs[i] = prs;
-                        // the force pass's per-neighbour factors p / rho^2 and 1 / rho
-                        a.dpr[i] = make_float2(prs / (rho * rho), 1.f / rho);
+                        // the force pass's neighbour records
+                        const float4 xi = a.pos[i];
+                        const float4 vi = a.vel[i];
+                        a.xq[i] = make_float4(xi.x, xi.y, xi.z, prs / (rho * rho));
+                        a.vq[i] = make_float4(vi.x, vi.y, vi.z, 1.f / rho);
                     } else if constexpr (KIND == PASS_FORCE) {
                         // compute_pressure_accel_n_normal_with_boundary: m * sum_fluid, then
                         // the boundary term (compute_pressure_accel_n_normal.cu:346-364)
@@ -929,6 +933,9 @@ __global__ void __launch_bounds__(WPB * 32, KindCfg<KIND>::min_warps / WPB) cell
                         const float sn = P.h * P.mass;
                         a.normal[i] = f4(sn * res[3], sn * res[4], sn * res[5]);
                         a.vlap[i] = f4(res[6], res[7], res[8]);
+                        // the surface pass's neighbour record
+                        const float4 xi = a.pos[i];
+                        a.xr[i] = make_float4(xi.x, xi.y, xi.z, a.rho[i]);
                     } else if constexpr (KIND == PASS_SURFACE) {
                         // a_np = g + F_ext + nu*10*m*vlap - alpha*2*rho0*f
                         const float4 xi = a.pos[i];

@@ -65,7 +65,10 @@ struct TravArgs {
     // fields
     float* rho;
     float* prs;
-    float2* dpr;              // (p / rho^2, 1 / rho), written by the density pass
+    // neighbour records packed for the gathers of the force and surface passes
+    float4* xq;               // (x, y, z, p / rho^2), written by the density pass
+    float4* vq;               // (vx, vy, vz, 1 / rho), written by the density pass
+    float4* xr;               // (x, y, z, rho), written by the force pass
     float4* ap;
     float4* normal;
     float4* vlap;
