@@ -54,6 +54,18 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
+def measured_traffic(workload: str, n: int, kernel: str):
+    """DRAM bytes per launch of `kernel` from the committed ncu capture of this
+    workload (profiles/dram_traffic_<workload>.json), or None."""
+    p = ROOT / "profiles" / f"dram_traffic_{workload}.json"
+    if not p.exists():
+        return None
+    d = json.loads(p.read_text())
+    if d.get("particles") != n:
+        return None
+    return d["bytes_per_launch"].get(kernel)
+
+
 class ClockSampler:
     """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
 
@@ -238,6 +250,7 @@ def run_ours(args, world, rank, local, dist):
         return None
     peak, peak_kind = measured_peaks()
     dom = max(("density_pass", "force_pass", "surface_integrate_pass"), key=lambda k: stage_ms.get(k, 0.0))
+    traffic = measured_traffic(args.workload, n, dom)
     dom_ms = stage_ms[dom]
     achieved = PASS_BYTES[dom] * n / (dom_ms * 1e-3) / 1e9
     value = world * n * args.steps / (ms_max * 1e-3)
@@ -257,7 +270,7 @@ def run_ours(args, world, rank, local, dist):
                 "d2h_bytes_per_step": d2h},
         "gpu_launches": launches,
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "peak_source": peak_kind, "traffic": None,
+                     "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic,
                      "stage_ms": stage_ms},
     }
     line.update(extras)
