@@ -75,7 +75,7 @@ struct WarpView {
 };
 
 template <int KIND>
-__host__ __device__ __forceinline__ size_t warp_smem_bytes(u32 cap, WarpView<KIND>* v = nullptr,
+__host__ __device__ __forceinline__ size_t warp_smem_bytes(u32 cap, bool with_boundary, WarpView<KIND>* v = nullptr,
                                                            unsigned char* base = nullptr) {
     using C = KindCfg<KIND>;
     size_t o = 0;
@@ -90,7 +90,7 @@ __host__ __device__ __forceinline__ size_t warp_smem_bytes(u32 cap, WarpView<KIN
     unsigned char* rstart = take(4ull * (MAX_RANGE_CELLS + 3));
     unsigned char* rpref = take(4ull * (MAX_RANGE_CELLS + 3));
     unsigned char *bcand = nullptr, *bstart = nullptr, *bpref = nullptr;
-    if (C::boundary) {
+    if (C::boundary && with_boundary) {   // only scenes with boundary particles
         bcand = take(4ull * BCAND_CAP);
         bstart = take(4ull * (MAX_BOUNDARY_CELLS + 3));
         bpref = take(4ull * (MAX_BOUNDARY_CELLS + 3));
@@ -695,8 +695,9 @@ __global__ void __launch_bounds__(WPB * 32, KindCfg<KIND>::min_warps / WPB) cell
     const u32 warp = threadIdx.x >> 5;
     const u32 cap = a.mask_words * 32u;
     WarpView<KIND> S;
-    const size_t wbytes = warp_smem_bytes<KIND>(cap);
-    warp_smem_bytes<KIND>(cap, &S, dyn_smem + warp * wbytes);
+    const bool with_boundary = a.nb > 0;
+    const size_t wbytes = warp_smem_bytes<KIND>(cap, with_boundary);
+    warp_smem_bytes<KIND>(cap, with_boundary, &S, dyn_smem + warp * wbytes);
 
     float dt = 0.f, np_dt = 0.f;
     if constexpr (KIND == PASS_SURFACE) {
@@ -1215,11 +1216,11 @@ void launch_reorder_cells(const float4* pos_in, const float4* vel_in, const u32*
 template <int KIND, int WPB, bool BATCH>
 static void launch_wpb(const DevParams& P, const TravArgs& a, cudaStream_t stream, u32 grid) {
     // per-warp candidate staging sized by the bit-matrix capacity 32 * mask_words
-    const size_t bytes = warp_smem_bytes<KIND>(a.mask_words * 32u) * WPB;
+    const size_t bytes = warp_smem_bytes<KIND>(a.mask_words * 32u, a.nb > 0) * WPB;
     static bool configured = false;  // per instantiation; the attribute is per device function
     if (!configured) {
         cudaFuncSetAttribute(cell_pass_kernel<KIND, WPB, BATCH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             static_cast<int>(warp_smem_bytes<KIND>(32u * MAX_MASK_WORDS) * WPB));
+                             static_cast<int>(warp_smem_bytes<KIND>(32u * MAX_MASK_WORDS, true) * WPB));
         configured = true;
     }
     cell_pass_kernel<KIND, WPB, BATCH><<<grid, WPB * 32, bytes, stream>>>(P, a);

@@ -125,13 +125,13 @@ def run_one_step(p, bx, pos, vel, bpos, delta, **sim_kw):
     return out
 
 
-def oracle_one_step(p, bx, pos, vel, bpos, delta):
+def oracle_one_step(p, bx, pos, vel, bpos, delta, nbr_cap=None):
     if bpos is not None and len(bpos):
         bs, bm = oracle.boundary_init(p, bpos)
     else:
         bs, bm = None, None
     n = pos.shape[0]
-    cap = n * min(max(n, 1), 1024)
+    cap = nbr_cap if nbr_cap is not None else n * min(max(n, 1), 1024)
     return oracle.step(p, bx, pos, vel, bs, bm, delta=delta, nbr_cap=cap), bs, bm
 
 

@@ -15,9 +15,9 @@ from parity import (check_fields, dam_break_scene, field_close, hash_cell_map, o
 pytestmark = pytest.mark.gpu
 
 
-def check_step(p, bx, pos, vel, bpos, delta, with_fields=True):
+def check_step(p, bx, pos, vel, bpos, delta, with_fields=True, nbr_cap=None):
     got = run_one_step(p, bx, pos, vel, bpos, delta)
-    ref, bs, bm = oracle_one_step(p, bx, pos, vel, bpos, delta)
+    ref, bs, bm = oracle_one_step(p, bx, pos, vel, bpos, delta, nbr_cap=nbr_cap)
     n = pos.shape[0]
     # integer work: bit-exact
     assert np.array_equal(got["morton_keys"], ref.keys), "Morton keys differ"
@@ -104,3 +104,13 @@ def test_dense_cell_many_home_batches():
     p = wcsph.default_params(particle_radius=0.01, max_time_step=1e-3, cfl_factor=0.0)
     bx = wcsph.box((0, 0, 0), (1, 1, 1))
     check_step(p, bx, pos, np.zeros_like(pos), None, 1e-3)
+
+
+def test_benchmark_scene_full_size():
+    """The 1,048,576-particle benchmark scene (tilting-box preset, r = 0.004,
+    jitter +-0.2 r, N(0, 0.1) velocities): one step at full size, every check
+    of the small scenes (33 M neighbour pairs compared bit-exact)."""
+    pre = wcsph.preset("large_tilting")
+    n = pre.info.fluid_n
+    assert n == 1 << 20
+    check_step(pre.params, pre.box, pre.pos, pre.vel, None, pre.info.delta, nbr_cap=n * 96)
