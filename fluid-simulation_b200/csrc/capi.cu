@@ -356,6 +356,14 @@ int wcsph_rollout_backward(wcsph_ctx* ctx, float* grad_v0, float* grad_viscosity
     return guarded(ctx, [&] { ctx->sim->rollout_backward(grad_v0, grad_viscosity, grad_stiffness); });
 }
 
+// ---- headless rendering --------------------------------------------------------
+int wcsph_render(wcsph_ctx* ctx, const wcsph_camera* cam, const wcsph_render_opts* opts, uint8_t* rgba,
+                 float* depth) {
+    CHECK_CTX(ctx);
+    if (!cam || !opts) return WCSPH_ERR_INVALID_ARGUMENT;
+    return guarded(ctx, [&] { ctx->sim->render(*cam, *opts, rgba, depth); });
+}
+
 // ---- allocation-free key sort ------------------------------------------------
 // No counterpart in the reference; for callers that cannot allocate device
 // memory while they run (see include/wcsph.h). Errors go to wcsph_last_error(NULL).

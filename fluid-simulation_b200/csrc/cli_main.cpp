@@ -3,6 +3,7 @@
 // Application::init/run_headless/stop_reached src/application.cu:24-58,105-161).
 // One executable serves every preset scene (--scene NAME) instead of one
 // executable per app; all other flags keep the reference's meaning.
+#include <algorithm>
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -32,6 +33,11 @@ struct RunOptions {
     std::string scene = "surface_tension";
     int device = -1;
     uint64_t seed = 0;
+    // headless frames of the particle view (the reference's window contents)
+    std::optional<std::string> frames_dir;
+    int frame_every = 10;
+    uint32_t frame_w = 640, frame_h = 480;
+    float camera[5] = {0.f, 0.f, 2.5f, 270.f, 0.f};   // x, y, z, yaw deg, pitch deg (application.cu:16)
 };
 
 void print_usage(const char* prog) {
@@ -51,7 +57,11 @@ void print_usage(const char* prog) {
                  "  --log-csv FILE                  Per-step CSV log\n"
                  "  --log-metrics                   Add mean_speed,ke columns\n"
                  "  --device N                      CUDA device (default: current)\n"
-                 "  --seed N                        Seed of the scene's jitter/velocities\n";
+                 "  --seed N                        Seed of the scene's jitter/velocities\n"
+                 "  --frames DIR                    Write the particle view as PPM frames into DIR\n"
+                 "  --frame-every N                 Frame interval in steps (default 10)\n"
+                 "  --frame-size WxH                Default 640x480\n"
+                 "  --camera x,y,z,yaw,pitch        Degrees; default 0,0,2.5,270,0\n";
 }
 
 int parse_searcher(const char* s) {
@@ -99,6 +109,18 @@ RunOptions parse_cli(int argc, char** argv) {
         else if (!std::strcmp(a, "--scene")) o.scene = need(i, a);
         else if (!std::strcmp(a, "--device")) o.device = std::atoi(need(i, a));
         else if (!std::strcmp(a, "--seed")) o.seed = std::strtoull(need(i, a), nullptr, 10);
+        else if (!std::strcmp(a, "--frames")) o.frames_dir = need(i, a);
+        else if (!std::strcmp(a, "--frame-every")) o.frame_every = std::max(1, std::atoi(need(i, a)));
+        else if (!std::strcmp(a, "--frame-size")) {
+            const char* v = need(i, a);
+            if (std::sscanf(v, "%ux%u", &o.frame_w, &o.frame_h) != 2 || !o.frame_w || !o.frame_h)
+                throw std::invalid_argument(std::string("bad --frame-size: ") + v);
+        } else if (!std::strcmp(a, "--camera")) {
+            const char* v = need(i, a);
+            if (std::sscanf(v, "%f,%f,%f,%f,%f", &o.camera[0], &o.camera[1], &o.camera[2], &o.camera[3],
+                            &o.camera[4]) != 5)
+                throw std::invalid_argument(std::string("bad --camera: ") + v);
+        }
         else if (!std::strcmp(a, "--help") || !std::strcmp(a, "-h")) { print_usage(argv[0]); std::exit(EXIT_SUCCESS); }
         else throw std::invalid_argument(std::string("Unknown argument: ") + a);
     }
@@ -183,6 +205,27 @@ struct App {
             if (opts.log_metrics) log << ",mean_speed,ke";
             log << '\n';
         }
+        wcsph_camera cam{};
+        wcsph_render_opts ropt{};
+        std::vector<uint8_t> rgba;
+        if (opts.frames_dir) {
+            const float deg = 3.14159265358979f / 180.f;
+            wcsph_camera_look(opts.camera, opts.camera[3] * deg, opts.camera[4] * deg, opts.frame_w, opts.frame_h, &cam);
+            wcsph_default_render_opts(&ropt);
+            ropt.width = opts.frame_w;
+            ropt.height = opts.frame_h;
+            ropt.radius = info.params.particle_radius;
+            rgba.resize(static_cast<size_t>(opts.frame_w) * opts.frame_h * 4);
+        }
+        auto write_frame = [&](int k) {
+            check(wcsph_render(ctx, &cam, &ropt, rgba.data(), nullptr), ctx, "render");
+            char name[64];
+            std::snprintf(name, sizeof(name), "/frame_%06d.ppm", k);
+            std::ofstream f(*opts.frames_dir + name, std::ios::binary);
+            if (!f) throw std::runtime_error("cannot write frame into " + *opts.frames_dir);
+            f << "P6\n" << opts.frame_w << ' ' << opts.frame_h << "\n255\n";
+            for (size_t px = 0; px < rgba.size(); px += 4) f.write(reinterpret_cast<const char*>(&rgba[px]), 3);
+        };
         while (!stop_reached(step, sim_time, t0)) {
             const auto ts = clock::now();
             update_objects(opts.fixed_dt);
@@ -200,6 +243,7 @@ struct App {
                 }
                 log << '\n';
             }
+            if (opts.frames_dir && step % opts.frame_every == 0) write_frame(step);
             ++step;
         }
         if (opts.snapshot_save) {

@@ -2,6 +2,7 @@
 // parity field export. Reference orchestration: CUDASPHSimulator::update
 // (src/cuda/SPH/sph.cu:31-60) -> StepTuner::launch (step_tuner.cuh:259-295).
 #include "simulator.cuh"
+#include "render.cuh"
 
 #include <algorithm>
 #include <bit>
@@ -614,6 +615,52 @@ int CUDASPHSimulator::kernel_timings(const char** names, float* ms, int cap) {
         if (ms) ms[s] = kernel_times_[s].second;
     }
     return k;
+}
+
+}  // namespace wcsph
+
+namespace wcsph {
+
+void CUDASPHSimulator::render(const wcsph_camera& cam, const wcsph_render_opts& o, uint8_t* rgba, float* depth) {
+    if (o.width == 0 || o.height == 0 || o.width > 16384 || o.height > 16384)
+        throw Error(WCSPH_ERR_INVALID_ARGUMENT, "render size must be 1..16384 per side");
+    if (!(o.radius > 0.f)) throw Error(WCSPH_ERR_INVALID_ARGUMENT, "render radius must be positive");
+    if (!rgba) throw Error(WCSPH_ERR_INVALID_ARGUMENT, "render needs an rgba buffer");
+    RenderArgs r{};
+    std::memcpy(r.proj, cam.projection, sizeof(r.proj));
+    std::memcpy(r.view, cam.view, sizeof(r.view));
+    mat4_mul(r.proj, r.view, r.vp);
+    if (!mat4_inverse(r.vp, r.inv_vp)) throw Error(WCSPH_ERR_INVALID_ARGUMENT, "camera matrices are singular");
+    std::memcpy(r.eye, cam.eye, sizeof(r.eye));
+    r.width = o.width;
+    r.height = o.height;
+    r.radius = o.radius;
+    r.show_boundary = o.show_boundary ? 1 : 0;
+    r.normalize = o.normalize ? 1 : 0;
+    r.min_value = o.min_value;
+    r.max_value = o.max_value;
+    std::memcpy(r.background, o.background, sizeof(r.background));
+    r.max_pixels = o.max_pixels > 0 ? o.max_pixels : (1 << 16);
+    const float* scalar = nullptr;
+    const float4* vec = nullptr;
+    switch (o.field) {
+    case -1: r.mode = RENDER_PLAIN; break;
+    case WCSPH_FIELD_DENSITY: case WCSPH_FIELD_PRESSURE:
+        r.mode = RENDER_SCALAR; scalar = static_cast<const float*>(device_field(o.field)); break;
+    case WCSPH_FIELD_VELOCITY: case WCSPH_FIELD_PRESSURE_ACCEL: case WCSPH_FIELD_NON_PRESSURE_ACCEL:
+    case WCSPH_FIELD_NORMAL:
+        r.mode = RENDER_VECTOR; vec = static_cast<const float4*>(device_field(o.field)); break;
+    default: throw Error(WCSPH_ERR_INVALID_ARGUMENT, "field cannot be visualised");
+    }
+    if (r.normalize && !(r.max_value != r.min_value)) throw Error(WCSPH_ERR_INVALID_ARGUMENT, "min_value == max_value");
+    const size_t npix = static_cast<size_t>(o.width) * o.height;
+    if (render_z_.count != npix) { render_z_.alloc(npix); render_rgba_.alloc(npix); render_depth_.alloc(npix); }
+    enqueue_render(r, pos_a_.ptr, n_, bpos_.ptr, nb_, scalar, vec, render_z_.ptr, render_rgba_.ptr,
+                   depth ? render_depth_.ptr : nullptr, stream_);
+    WCSPH_CUDA(cudaGetLastError());
+    WCSPH_CUDA(cudaMemcpyAsync(rgba, render_rgba_.ptr, npix * 4, cudaMemcpyDeviceToHost, stream_));
+    if (depth) WCSPH_CUDA(cudaMemcpyAsync(depth, render_depth_.ptr, npix * sizeof(float), cudaMemcpyDeviceToHost, stream_));
+    synchronize();
 }
 
 }  // namespace wcsph

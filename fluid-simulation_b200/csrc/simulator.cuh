@@ -126,6 +126,7 @@ public:
 
     int kernel_timings(const char** names, float* ms, int cap);
     int launches_per_step() const;
+    void render(const wcsph_camera& cam, const wcsph_render_opts& o, uint8_t* rgba, float* depth);
 
     // tuning
     const StepConfig& config() const { return cfg_; }
@@ -190,6 +191,9 @@ private:
     DevBuf<float4> xq_, vq_, xr_;
     DevBuf<float4> ap_, normal_, vlap_, anp_;
     DevBuf<float> partials_;
+    DevBuf<unsigned long long> render_z_;
+    DevBuf<u32> render_rgba_;
+    DevBuf<float> render_depth_;
     DevBuf<u32> group_done_;
     DevBuf<double> group_partials_;
     DevBuf<DevState> st_;

@@ -100,6 +100,18 @@ class Scene(C.Structure):
                 ("boundary_pos", C.POINTER(C.c_float)), ("box", Box)]
 
 
+class Camera(C.Structure):
+    """wcsph_camera: column-major projection and view matrices, eye position."""
+    _fields_ = [("projection", C.c_float * 16), ("view", C.c_float * 16), ("eye", C.c_float * 3)]
+
+
+class RenderOpts(C.Structure):
+    _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("radius", C.c_float),
+                ("show_boundary", C.c_int), ("field", C.c_int), ("normalize", C.c_int),
+                ("min_value", C.c_float), ("max_value", C.c_float), ("background", C.c_float * 3),
+                ("max_pixels", C.c_int)]
+
+
 class PresetInfo(C.Structure):
     _fields_ = [("params", Params), ("box", Box), ("fluid_n", C.c_uint32), ("boundary_n", C.c_uint32),
                 ("delta", C.c_float), ("steps", C.c_int32), ("sim_time", C.c_float), ("moving_box", C.c_int32)]
@@ -183,6 +195,9 @@ def load_library(path: str | os.PathLike | None = None) -> C.CDLL:
         "wcsph_rollout_forward": (C.c_int, [vp, C.c_int, C.c_float, C.c_int, f, f]),
         "wcsph_rollout_backward": (C.c_int, [vp, f, f, f]),
         "wcsph_sort_keys_static": (C.c_int, [vp, C.c_uint32, vp, vp]),
+        "wcsph_camera_look": (None, [f, C.c_float, C.c_float, C.c_uint32, C.c_uint32, C.POINTER(Camera)]),
+        "wcsph_default_render_opts": (None, [C.POINTER(RenderOpts)]),
+        "wcsph_render": (C.c_int, [vp, C.POINTER(Camera), C.POINTER(RenderOpts), vp, f]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -336,6 +351,35 @@ def _check(status: int, ctx, lib=None):
                   ERR_SNAPSHOT_TRUNCATED) or (status == ERR_IO and "Snapshot" in msg):
         raise SnapshotError(status, msg)
     raise WcsphError(status, msg or lib.wcsph_status_string(status).decode())
+
+
+def camera_look(position=(0.0, 0.0, 2.5), yaw=np.radians(270.0), pitch=0.0, width=640, height=480) -> Camera:
+    """The reference's Camera(position, yaw, pitch, width, height); the default
+    is its start view (src/application.cu:16)."""
+    cam = Camera()
+    pos = (C.c_float * 3)(*[float(x) for x in position])
+    load_library().wcsph_camera_look(pos, float(yaw), float(pitch), width, height, C.byref(cam))
+    return cam
+
+
+def render_opts(**kw) -> RenderOpts:
+    o = RenderOpts()
+    load_library().wcsph_default_render_opts(C.byref(o))
+    for k, v in kw.items():
+        if k == "field" and isinstance(v, str):
+            v = FIELD[v]
+        if k == "background":
+            v = (C.c_float * 3)(*v)
+        setattr(o, k, v)
+    return o
+
+
+def write_ppm(path, rgba: np.ndarray) -> None:
+    """Binary PPM (P6) of an RGBA image [H, W, 4]."""
+    h, w = rgba.shape[:2]
+    with open(path, "wb") as fh:
+        fh.write(b"P6\n%d %d\n255\n" % (w, h))
+        fh.write(np.ascontiguousarray(rgba[..., :3]).tobytes())
 
 
 STATIC_SORT_MAX_KEYS = 65536
@@ -504,6 +548,15 @@ class CUDASPHSimulator:
         ms = C.c_float()
         self._c(self._lib.wcsph_time_steps(self._ctx, n, delta, C.byref(ms)))
         return ms.value
+
+    def render(self, camera: Camera, opts: RenderOpts | None = None, with_depth: bool = False):
+        """Headless particle view of the current state -> rgba [H, W, 4] (and depth [H, W])."""
+        o = opts or render_opts()
+        rgba = np.empty((o.height, o.width, 4), np.uint8)
+        depth = np.empty((o.height, o.width), np.float32) if with_depth else None
+        self._c(self._lib.wcsph_render(self._ctx, C.byref(camera), C.byref(o), rgba.ctypes.data_as(C.c_void_p),
+                                       fptr(depth)))
+        return (rgba, depth) if with_depth else rgba
 
     def kernel_timings(self):
         names = (C.c_char_p * 16)()

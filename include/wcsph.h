@@ -325,6 +325,41 @@ int wcsph_rollout_forward(wcsph_ctx* ctx, int steps, float dt, int checkpoint_ev
 int wcsph_rollout_backward(wcsph_ctx* ctx, float* grad_v0, float* grad_viscosity,
                            float* grad_stiffness);
 
+/* ---- headless particle rendering ------------------------------------------
+ * The reference's particle view (shaders/instanced_ball.vert:20-32 and
+ * instanced_ball.frag: camera-facing quads shaded as spheres, fluid blue,
+ * boundary orange, optional field visualisation) computed by CUDA kernels
+ * into an RGBA8 image, without a graphics stack. Matrices are column-major
+ * (glm layout); image row 0 is the top row.                                 */
+typedef struct wcsph_camera {
+    float projection[16];
+    float view[16];
+    float eye[3];
+} wcsph_camera;
+/* Camera(position, yaw, pitch, width, height) of src/render/camera.cpp:7-33:
+ * perspective 45 deg, near 0.1, far 100, world up (0, 1, 0). The reference's
+ * start view is position (0, 0, 2.5), yaw 270 deg, pitch 0 (angles in radians). */
+void wcsph_camera_look(const float position[3], float yaw, float pitch, uint32_t width, uint32_t height,
+                       wcsph_camera* out);
+typedef struct wcsph_render_opts {
+    uint32_t width, height;
+    float radius;            /* sphere radius (the shaders' RADIUS 0.02)         */
+    int show_boundary;       /* draw boundary particles                          */
+    int field;               /* -1: plain colours; WCSPH_FIELD_DENSITY or _PRESSURE
+                                (grey = value); WCSPH_FIELD_VELOCITY, _PRESSURE_ACCEL,
+                                _NON_PRESSURE_ACCEL or _NORMAL (colour * dot(v, n)),
+                                on fluid particles                               */
+    int normalize;           /* map [min_value, max_value] to [0, 1]             */
+    float min_value, max_value;
+    float background[3];
+    int max_pixels;          /* skip particles whose quad covers more pixels     */
+} wcsph_render_opts;
+void wcsph_default_render_opts(wcsph_render_opts* o);
+/* Renders the current state: rgba (width*height*4 bytes) and, if not NULL,
+ * depth (width*height floats, window depth in [0, 1], 1 = background).     */
+int wcsph_render(wcsph_ctx* ctx, const wcsph_camera* cam, const wcsph_render_opts* opts, uint8_t* rgba,
+                 float* depth);
+
 /* ---- allocation-free key sort ---------------------------------------------
  * No counterpart in the reference (its sort is thrust::sort_by_key, which
  * allocates temporary storage on every call).
