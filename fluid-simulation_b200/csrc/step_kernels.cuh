@@ -4,8 +4,9 @@
 //   reorder_cells   gather pos/vel into sorted order + mark cell runs + insert
 //                   cells into the linear-probed hash (cell_start/cell_end)
 //                   (particle_data.cuh:130-131 + rebuild_n_search.cu:10-36)
-//   density pass    rho, Tait p (+boundary) and the per-particle neighbour
-//                   bitmasks over the home cell's candidate list
+//   density pass    rho, Tait p (+boundary), the cell's neighbour bit matrix
+//                   over its candidate list and the packed neighbour records
+//                   of the force pass
 //                   (compute_rho_p[_with_boundary], compute_rho_p.cu:192-318)
 //   force pass      pressure accel (+boundary), normals, viscosity Laplacian
 //                   (compute_pressure_accel_n_normal.cu:240-366 and the
@@ -20,21 +21,22 @@
 // up the (2R+1)^3 neighbour cells once (lane-parallel hash probes) and
 // stages their particles (the candidates, in the reference's cell order)
 // into shared memory. The home particles are taken in blocks of up to 32.
-// A block's work is a flat item space split into 32 contiguous lane runs,
-// so every lane does the same amount of work whatever the home count:
-//   density pass   items = (home, candidate) pairs; the distance test
-//                  writes the cell's neighbour bit matrix (row = home
-//                  particle, bit = candidate, row-major in the cell's
-//                  mask_words * n_home words of the mask buffer);
-//   later passes   items = the set bits of that matrix (neighbours only).
-// Each lane keeps one partial sum per home row it crosses; the partials are
+// Every lane does the same amount of work whatever the home count:
+//   density pass   phase 1: each lane builds whole words of the block's
+//                  neighbour bit matrix (row = home particle, bit =
+//                  candidate; rows padded to whole words), testing two
+//                  candidates per packed-FP32 step; phase 2 sums W over the
+//                  set bits. The matrix is kept row-major in the cell's
+//                  mask_words * n_home words of the mask buffer;
+//   later passes   walk the set bits of that matrix (neighbours only).
+// The walks split the block's set bits into 32 contiguous lane runs; each
+// lane keeps one partial sum per home row it crosses and the partials are
 // added per home in lane order, so results are deterministic.
 #pragma once
 #include "sph_common.cuh"
 
 namespace wcsph {
 
-constexpr int TRAV_WARPS = 4;            // warps per block of the traversal passes
 constexpr int MAX_RANGE_CELLS = 125;     // (2R+1)^3 with R <= 2
 constexpr int MAX_BOUNDARY_CELLS = 125;
 constexpr u32 MAX_MASK_WORDS = 16;      // bit-matrix words per particle (candidate cap = 32 * words)
