@@ -482,10 +482,18 @@ class CUDASPHSimulator:
         self._c(self._lib.wcsph_set_params(self._ctx, C.byref(p)))
         self.params = p
 
-    def get_state(self):
+    def get_state(self, out=None):
+        """(positions, velocities) float32 [n, 4] in the current order; `out`
+        = (pos, vel) arrays to fill (e.g. views of pinned host memory)."""
         n = self.get_fluid_particles()
-        pos = np.empty((n, 4), np.float32)
-        vel = np.empty((n, 4), np.float32)
+        if out is None:
+            pos = np.empty((n, 4), np.float32)
+            vel = np.empty((n, 4), np.float32)
+        else:
+            pos, vel = out
+            for a in (pos, vel):
+                if a.shape != (n, 4) or a.dtype != np.float32 or not a.flags.c_contiguous:
+                    raise ValueError("out arrays must be contiguous float32 [n, 4]")
         self._c(self._lib.wcsph_get_state(self._ctx, fptr(pos), fptr(vel)))
         return pos, vel
 
