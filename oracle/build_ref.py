@@ -46,6 +46,11 @@ VARIANTS = {
     # scene (measurements/configs/BIG_falling.json: all blocks 32,
     # TABLE_SIZE_MULT 4, CELL_SIZE_MULT 1.0, neighbour lists, no smem)
     "large_tilting": dict(n=1048576, nb=0, r=0.004, k=("textbook", 1000.0), nu=0.01, max_dt=5e-4, cfl=0.0, table_mult=4, block=32),
+    # the same scene at the other block sizes of the reference tuner's space
+    # (step_tuner.cuh:331: 32, 64, 128, 256, 512)
+    # (the reference arm of bench.py reports the fastest)
+    **{f"large_tilting_b{b}": dict(n=1048576, nb=0, r=0.004, k=("textbook", 1000.0), nu=0.01, max_dt=5e-4, cfl=0.0,
+                                   table_mult=4, block=b) for b in (64, 128, 256, 512)},
     # 32^3 dam break with walls (dragon_settled.json: blocks 32, TABLE_SIZE_MULT 32)
     "dam_break": dict(n=32768, nb=7802, r=0.01, k=("textbook", 1000.0), nu=0.01, max_dt=1e-3, cfl=0.0, table_mult=32, block=32),
     # golden fixtures (2048 particles)

@@ -111,34 +111,71 @@ class RefSim:
         self.L.ref_destroy()
 
 
+_TIME_VARIANT = r"""
+import json, sys, time
+sys.path[:0] = [sys.argv[1], sys.argv[1] + '/../fluid-simulation_b200']
+import refpath, wcsph
+variant, workload, warmup, steps, seed = sys.argv[2], sys.argv[3], int(sys.argv[4]), int(sys.argv[5]), int(sys.argv[6])
+pre = wcsph.preset(workload, seed=seed)
+total = warmup + steps
+boxes = [pre.box_at(k + 1) for k in range(total)] if pre.info.moving_box else None
+sim = refpath.RefSim(variant, pre.pos, pre.vel, pre.bpos, pre.box, device=0)
+sim.time_steps(warmup, pre.info.delta, None if boxes is None else boxes[:warmup])
+t0 = time.perf_counter()
+ms = sim.time_steps(steps, pre.info.delta, None if boxes is None else boxes[warmup:total])
+wall = time.perf_counter() - t0
+sim.close()
+print(json.dumps({"ms": ms, "wall": wall}))
+"""
+
+
 def bench_line(args, metric: str) -> dict:
-    """`bench.py --impl reference`: the reference CUDA path on the same workload."""
+    """`bench.py --impl reference`: the reference CUDA path on the same workload.
+
+    Every built block size of the reference tuner's space (the frozen config
+    of its largest shipped scene uses 32; variants `<workload>_b<block>`) runs
+    the same warm-up + timed steps from the same initial state, each in a
+    process of its own (every harness library carries its own CUDA runtime
+    and Thrust); the fastest is the line's value and all are listed."""
+    import subprocess
+
     sys.path.insert(0, str(HERE.parent / "fluid-simulation_b200"))
     import wcsph
 
-    variant = args.workload
-    if not available(variant):
-        return {"impl": "reference", "unavailable": f"reference harness for {variant} not built "
+    variants = [v for v in [args.workload] + [f"{args.workload}_b{b}" for b in (64, 128, 256, 512)] if available(v)]
+    if not variants:
+        return {"impl": "reference", "unavailable": f"reference harness for {args.workload} not built "
                                                     f"(oracle/build_ref.py needs the reference sources)"}
     pre = wcsph.preset(args.workload, seed=args.seed)
     n = pre.info.fluid_n
     delta = pre.info.delta
-    total = args.warmup + args.steps
-    boxes = [pre.box_at(k + 1) for k in range(total)] if pre.info.moving_box else None
-    sim = RefSim(variant, pre.pos, pre.vel, pre.bpos, pre.box, device=0)
-    sim.time_steps(args.warmup, delta, None if boxes is None else boxes[: args.warmup])
-    t0 = time.perf_counter()
-    ms = sim.time_steps(args.steps, delta, None if boxes is None else boxes[args.warmup:total])
-    wall = time.perf_counter() - t0
-    sim.close()
+    sweep = {}
+    best = None
+    for variant in variants:
+        block = 32 if variant == args.workload else int(variant.rsplit("_b", 1)[1])
+        r = subprocess.run([sys.executable, "-c", _TIME_VARIANT, str(HERE), variant, args.workload,
+                            str(args.warmup), str(args.steps), str(args.seed)],
+                           capture_output=True, text=True, timeout=900)
+        if r.returncode != 0 or not r.stdout.strip():
+            sweep[str(block)] = f"failed (exit {r.returncode})"
+            continue
+        t = json.loads(r.stdout.strip().splitlines()[-1])
+        sweep[str(block)] = t["ms"] / args.steps
+        if best is None or t["ms"] < best[0]:
+            best = (t["ms"], t["wall"], block)
+    if best is None:
+        return {"impl": "reference", "unavailable": f"every reference harness variant failed: {sweep}"}
+    ms, wall, block = best
     value = n * args.steps / (ms * 1e-3)
     return {
         "impl": "reference", "metric": metric, "value": value, "unit": metric, "n_gpus": 1, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (same preset as --impl ours)",
         "config": {"workload": args.workload, "particles": n, "dt": delta,
-                   "reference_path": "reference kernels (src/cuda/tuning/kernels, frozen config of the "
-                                     "largest shipped scene) + Thrust sort/gather/scan/reduce, host CFL readback"},
+                   "reference_path": "reference kernels (src/cuda/tuning/kernels; neighbour lists, table mult 4, "
+                                     "cell mult 1 as in the largest shipped scene's frozen config) + Thrust "
+                                     "sort/gather/scan/reduce, host CFL readback",
+                   "block": block, "ms_per_step_by_block": sweep},
         "cpu_baseline": {"value": value, "unit": metric, "cores": 0, "kind": "reference",
                          "sample": f"{args.steps} steps of the reference CUDA path (the reference has no CPU solver)"},
         "e2e": {"value": n * args.steps / wall, "unit": metric, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
