@@ -15,10 +15,11 @@ __device__ __forceinline__ u32 lanemask_lt() {
 // Warp-aggregated shared-memory increment of 8 digit histograms for one key
 // per lane. Many lanes share digits (keys arrive nearly sorted), so each
 // distinct digit value gets one atomic.
-__device__ __forceinline__ void hist_add_key(u32 (*s_hist)[256], u64 key, bool valid) {
+__device__ __forceinline__ void hist_add_key(u32 (*s_hist)[256], u64 key, bool valid, int ndigits = SORT_DIGITS) {
     const u32 lane = threadIdx.x & 31;
 #pragma unroll
     for (int p = 0; p < SORT_DIGITS; ++p) {
+        if (p >= ndigits) break;   // uniform across the grid
         const u32 d = valid ? static_cast<u32>((key >> (8 * p)) & 255u) : 256u;
         const u32 peers = __match_any_sync(0xffffffffu, d);
         const u32 leader = __ffs(peers) - 1;
@@ -53,6 +54,74 @@ __global__ void keys_hist_kernel(const float4* __restrict__ pos, u32 n, float cs
         }
         hist_add_key(s_hist, key, valid);
     }
+    __syncthreads();
+    flush_hist(s_hist, hist);
+}
+
+__global__ void keys_bounds_kernel(const float4* __restrict__ pos, u32 n, float cs, u64* __restrict__ keys_out,
+                                   DevState* __restrict__ st) {
+    int lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+    for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int3 c = cell_of(pos[i], cs);
+        keys_out[i] = morton_key(c);
+        lo[0] = min(lo[0], c.x); hi[0] = max(hi[0], c.x);
+        lo[1] = min(lo[1], c.y); hi[1] = max(hi[1], c.y);
+        lo[2] = min(lo[2], c.z); hi[2] = max(hi[2], c.z);
+    }
+    // warp, then block, then one atomic per axis and block
+    __shared__ int s_lo[3], s_hi[3];
+    if (threadIdx.x < 3) { s_lo[threadIdx.x] = 0; s_hi[threadIdx.x] = 0; }
+    __syncthreads();
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        lo[d] = __reduce_min_sync(0xffffffffu, lo[d]);
+        hi[d] = __reduce_max_sync(0xffffffffu, hi[d]);
+    }
+    if ((threadIdx.x & 31) == 0) {
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            atomicMin(&s_lo[d], lo[d]);
+            atomicMax(&s_hi[d], hi[d]);
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x < 3) {
+        if (s_lo[threadIdx.x] < 0) atomicMin(&st->cell_lo[threadIdx.x], s_lo[threadIdx.x]);
+        if (s_hi[threadIdx.x] > 0) atomicMax(&st->cell_hi[threadIdx.x], s_hi[threadIdx.x]);
+    }
+}
+
+__global__ void compressed_keys_hist_kernel(const float4* __restrict__ pos, u32 n, float cs,
+                                            const DevState* __restrict__ st, u64* __restrict__ ckeys,
+                                            u32* __restrict__ hist) {
+    __shared__ u32 s_hist[SORT_DIGITS][256];
+    for (int t = threadIdx.x; t < SORT_DIGITS * 256; t += blockDim.x) (&s_hist[0][0])[t] = 0;
+    // smallest B with every cell coordinate in [-2^B, 2^B); B = 20 is the full key
+    const int lo = min(st->cell_lo[0], min(st->cell_lo[1], st->cell_lo[2]));
+    const int hi = max(st->cell_hi[0], max(st->cell_hi[1], st->cell_hi[2]));
+    int B = 0;
+    while (B < 20 && !(lo >= -(1 << B) && hi < (1 << B))) ++B;
+    const int ndigits = (3 * (B + 1) + 7) / 8;   // digits above are 0 for every key
+    u32 valid_keys = 0;
+    __syncthreads();
+    const u32 stride = gridDim.x * blockDim.x;
+    for (u32 base = blockIdx.x * blockDim.x; base < n; base += stride) {   // uniform trip count (match.any)
+        const u32 i = base + threadIdx.x;
+        const bool valid = i < n;
+        u64 key = 0;
+        if (valid) {
+            const int3 c = cell_of(pos[i], cs);
+            key = part_by_3(static_cast<u32>(c.x + (1 << B))) | (part_by_3(static_cast<u32>(c.y + (1 << B))) << 1) |
+                  (part_by_3(static_cast<u32>(c.z + (1 << B))) << 2);
+            ckeys[i] = key;
+            ++valid_keys;
+        }
+        hist_add_key(s_hist, key, valid, ndigits);
+    }
+    // the digits above ndigits: every key in bucket 0
+    for (int o = 16; o > 0; o >>= 1) valid_keys += __shfl_xor_sync(0xffffffffu, valid_keys, o);
+    if ((threadIdx.x & 31) == 0 && valid_keys)
+        for (int p = ndigits; p < SORT_DIGITS; ++p) atomicAdd(&s_hist[p][0], valid_keys);
     __syncthreads();
     flush_hist(s_hist, hist);
 }
@@ -118,6 +187,7 @@ __global__ void sort_plan_kernel(u32 n, u32* __restrict__ hist, u32* __restrict_
         }
         st->sort_sel[SORT_DIGITS] = sel;
         st->first_active = first;
+        for (int d = 0; d < 3; ++d) st->cell_lo[d] = st->cell_hi[d] = 0;   // for the next sort
     }
 }
 

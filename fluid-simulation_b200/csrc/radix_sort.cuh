@@ -47,6 +47,22 @@ struct SortBuffers {
 __global__ void keys_hist_kernel(const float4* __restrict__ pos, u32 n, float cs,
                                  u64* __restrict__ keys_out, u32* __restrict__ hist,
                                  const u32* __restrict__ scene = nullptr);
+// The per-step keys of a single scene, in two arrays:
+//  * keys_bounds_kernel writes the reference's 63-bit Morton keys (the
+//    MORTON_KEYS field) and folds the cell-coordinate bounds into st;
+//  * compressed_keys_hist_kernel writes order-equivalent short keys for the
+//    sort and their digit histograms. With every cell coordinate c in
+//    [-2^B, 2^B), the offset coordinate u = c + 2^20 has bits B..19 equal to
+//    NOT bit 20, so those bits never decide a Morton comparison; v = c + 2^B
+//    keeps exactly bits 0..B-1 and bit 20 (as bit B), and Morton(v) orders any
+//    two particles as Morton(u) does. A scene of 125 x 63 x 63 cells around
+//    the origin needs 24 bits (3 digit passes) instead of 63 (8 passes); the
+//    stable sort gives the same permutation.
+__global__ void keys_bounds_kernel(const float4* __restrict__ pos, u32 n, float cs, u64* __restrict__ keys_out,
+                                   DevState* __restrict__ st);
+__global__ void compressed_keys_hist_kernel(const float4* __restrict__ pos, u32 n, float cs,
+                                            const DevState* __restrict__ st, u64* __restrict__ ckeys,
+                                            u32* __restrict__ hist);
 // Histograms of already-computed keys (boundary sort, re-sorts).
 __global__ void hist_only_kernel(const u64* __restrict__ keys, u32 n, u32* __restrict__ hist);
 __global__ void sort_plan_kernel(u32 n, u32* __restrict__ hist, u32* __restrict__ offsets,

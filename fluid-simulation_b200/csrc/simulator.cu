@@ -153,7 +153,7 @@ void CUDASPHSimulator::allocate() {
     hist_.alloc(SORT_DIGITS * 256);
     offsets_.alloc(SORT_DIGITS * 256);
     lookback_.alloc(static_cast<size_t>(SORT_DIGITS) * sort_tiles(n_) * 256);
-    perm_.alloc(n); ckey_.alloc(n);
+    perm_.alloc(n); ckey_.alloc(n); ckeys_.alloc(n);
     rho_.alloc(n); prs_.alloc(n); xq_.alloc(n); vq_.alloc(n); xr_.alloc(n);
     ap_.alloc(n); normal_.alloc(n); vlap_.alloc(n); anp_.alloc(n);
     st_.alloc(1); box_dev_.alloc(1); metrics_dev_.alloc(2);
@@ -283,17 +283,24 @@ TravArgs CUDASPHSimulator::trav_args(float delta) {
 void CUDASPHSimulator::enqueue_search(bool keys_from_state) {
     const u32 n = n_;
     WCSPH_CUDA(cudaMemsetAsync(table_.ptr, 0xff, table_.bytes(), stream_));
-    if (keys_from_state) {
-        keys_hist_kernel<<<std::min<u32>((n + 255) / 256, 1184), 256, 0, stream_>>>(pos_a_.ptr, n, dp_.cell_size,
-                                                                                    keys_[0].ptr, hist_.ptr);
-    }
+    if (keys_from_state) enqueue_keys();
     SortBuffers sb{};
     for (int i = 0; i < 3; ++i) { sb.keys[i] = keys_[i].ptr; sb.vals[i] = vals_[i].ptr; }
+    sb.keys[0] = ckeys_.ptr;   // the sort reads the compressed keys; keys_[0] keeps the field
     sb.hist = hist_.ptr; sb.offsets = offsets_.ptr; sb.lookback = lookback_.ptr; sb.capacity = n;
     enqueue_sort_passes(sb, n, st_.ptr, stream_);
     launch_reorder_cells(pos_a_.ptr, vel_a_.ptr, vals_[1].ptr, vals_[2].ptr, st_.ptr, n, dp_.cell_size, pos_b_.ptr,
                          vel_b_.ptr, perm_.ptr, ckey_.ptr, table_.ptr, cstart_.ptr, cend_.ptr, table_size_ - 1,
                          st_.ptr, stream_);
+}
+
+void CUDASPHSimulator::enqueue_keys() {
+    const u32 n = n_;
+    // few blocks: each flushes its histograms / bounds with global atomics on shared addresses
+    const u32 blocks = std::min<u32>((n + 255) / 256, 296);
+    keys_bounds_kernel<<<blocks, 256, 0, stream_>>>(pos_a_.ptr, n, dp_.cell_size, keys_[0].ptr, st_.ptr);
+    compressed_keys_hist_kernel<<<blocks, 256, 0, stream_>>>(pos_a_.ptr, n, dp_.cell_size, st_.ptr, ckeys_.ptr,
+                                                             hist_.ptr);
 }
 
 TravArgs CUDASPHSimulator::fixed_args(float dt) {
@@ -321,8 +328,8 @@ void CUDASPHSimulator::enqueue_step(float delta) {
 }
 
 int CUDASPHSimulator::launches_per_step() const {
-    // keys_hist + sort_plan + 8 onesweep + reorder_cells + 3 cell passes
-    return 1 + 1 + SORT_DIGITS + 1 + 3;
+    // keys_bounds + compressed_keys_hist + sort_plan + 8 onesweep + reorder_cells + 3 cell passes
+    return 2 + 1 + SORT_DIGITS + 1 + 3;
 }
 
 void CUDASPHSimulator::invalidate_graph() {
@@ -580,11 +587,11 @@ int CUDASPHSimulator::kernel_timings(const char** names, float* ms, int cap) {
     const u32 n = n_;
     WCSPH_CUDA(cudaEventRecord(ev[0], stream_));
     WCSPH_CUDA(cudaMemsetAsync(table_.ptr, 0xff, table_.bytes(), stream_));
-    keys_hist_kernel<<<std::min<u32>((n + 255) / 256, 1184), 256, 0, stream_>>>(pos_a_.ptr, n, dp_.cell_size,
-                                                                                keys_[0].ptr, hist_.ptr);
+    enqueue_keys();
     WCSPH_CUDA(cudaEventRecord(ev[1], stream_));
     SortBuffers sb{};
     for (int i = 0; i < 3; ++i) { sb.keys[i] = keys_[i].ptr; sb.vals[i] = vals_[i].ptr; }
+    sb.keys[0] = ckeys_.ptr;
     sb.hist = hist_.ptr; sb.offsets = offsets_.ptr; sb.lookback = lookback_.ptr; sb.capacity = n;
     enqueue_sort_passes(sb, n, st_.ptr, stream_);
     WCSPH_CUDA(cudaEventRecord(ev[2], stream_));

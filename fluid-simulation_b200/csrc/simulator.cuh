@@ -127,6 +127,8 @@ public:
     int kernel_timings(const char** names, float* ms, int cap);
     int launches_per_step() const;
     void render(const wcsph_camera& cam, const wcsph_render_opts& o, uint8_t* rgba, float* depth);
+    // Full Morton keys (field), cell bounds and the compressed keys + histograms.
+    void enqueue_keys();
 
     // tuning
     const StepConfig& config() const { return cfg_; }
@@ -189,6 +191,7 @@ private:
     DevBuf<u32> mask_;
     DevBuf<float> rho_, prs_;
     DevBuf<float4> xq_, vq_, xr_;
+    DevBuf<u64> ckeys_;         // order-equivalent short sort keys (radix_sort.cuh)
     DevBuf<float4> ap_, normal_, vlap_, anp_;
     DevBuf<float> partials_;
     DevBuf<unsigned long long> render_z_;

@@ -280,6 +280,10 @@ struct DevState {
     u32 sort_tile_counter[8];
     u32 first_active;           // first active pass (generates the iota values)
     u32 pad1[2];
+    // cell-coordinate bounds of the particles of the current sort (0 is always
+    // included; reset to 0 by the sort plan): they choose the compressed keys
+    int cell_lo[3];
+    int cell_hi[3];
 };
 
 enum : u32 {
