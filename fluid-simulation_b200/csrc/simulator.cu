@@ -136,6 +136,9 @@ CUDASPHSimulator::~CUDASPHSimulator() {
         cudaStreamSynchronize(stream_);
         cudaStreamDestroy(stream_);
     }
+    for (cudaEvent_t e : box_done_)
+        if (e) cudaEventDestroy(e);
+    if (box_pinned_) cudaFreeHost(box_pinned_);
     tuner_.reset();
 }
 
@@ -401,7 +404,16 @@ void CUDASPHSimulator::synchronize() {
 
 void CUDASPHSimulator::set_box(const wcsph_box& box) {
     box_host_ = make_dev_box(box);
-    WCSPH_CUDA(cudaMemcpyAsync(box_dev_.ptr, &box_host_, sizeof(DevBox), cudaMemcpyHostToDevice, stream_));
+    if (!box_pinned_) {
+        WCSPH_CUDA(cudaMallocHost(&box_pinned_, sizeof(DevBox) * kBoxSlots));
+        for (cudaEvent_t& e : box_done_) WCSPH_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    }
+    const int k = box_slot_;
+    box_slot_ = (box_slot_ + 1) % kBoxSlots;
+    WCSPH_CUDA(cudaEventSynchronize(box_done_[k]));   // returns at once for a never-recorded event
+    box_pinned_[k] = box_host_;
+    WCSPH_CUDA(cudaMemcpyAsync(box_dev_.ptr, box_pinned_ + k, sizeof(DevBox), cudaMemcpyHostToDevice, stream_));
+    WCSPH_CUDA(cudaEventRecord(box_done_[k], stream_));
 }
 
 void CUDASPHSimulator::set_params(const wcsph_params& p) {

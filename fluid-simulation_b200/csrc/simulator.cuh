@@ -201,6 +201,13 @@ private:
     DevBuf<double> group_partials_;
     DevBuf<DevState> st_;
     DevBuf<DevBox> box_dev_;
+    // Box uploads between steps go through a small pinned ring so that the
+    // copy is truly asynchronous (a pageable source may make the driver wait
+    // for the stream); slot k is reused only after its last copy completed.
+    static constexpr int kBoxSlots = 16;
+    DevBox* box_pinned_ = nullptr;
+    cudaEvent_t box_done_[kBoxSlots] = {};
+    int box_slot_ = 0;
     DevBuf<float> metrics_dev_;
     // boundary
     DevBuf<float4> bpos_;
