@@ -69,6 +69,7 @@ struct BatchSim {
     DevBuf<u32> hist, offs, lookback, perm;
     DevBuf<u64> ckey, table;
     DevBuf<u32> cstart, cend, mask;
+    DevBuf<u32> nbr, nbr_cnt;          // neighbour lists, nbr_width slots per particle
     u32 table_size = 0;
     DevBuf<float> rho, prs, partials, metric_sums;
     DevBuf<u32> group_done;
@@ -83,6 +84,7 @@ struct BatchSim {
     DevBuf<u32> bcstart, bcend;
     u32 btable_size = 0;
     int mask_words = 10;
+    int nbr_width = 64;
 
     cudaGraphExec_t graph = nullptr;
     float graph_delta = -1.f;
@@ -111,6 +113,9 @@ struct BatchSim {
         a.mask = mask.ptr;
         a.mask_words = static_cast<u32>(mask_words);
         a.chunk = n < (1u << 18) ? 8u : 32u;
+        a.nbr = nbr_width > 0 ? nbr.ptr : nullptr;
+        a.nbr_cnt = nbr_cnt.ptr;
+        a.nbr_width = static_cast<u32>(nbr_width);
         a.rho = rho.ptr; a.prs = prs.ptr;
         a.xq = xq.ptr; a.vq = vq.ptr; a.xr = xr.ptr;
         a.ap = ap.ptr; a.normal = normal.ptr; a.vlap = vlap.ptr; a.anp = anp.ptr;
@@ -251,6 +256,9 @@ static void build_batch(BatchSim& B, const wcsph_params& p, const wcsph_batch_sc
     B.table_size = static_cast<u32>(std::max<u64>(std::bit_ceil(static_cast<u64>(n)) / 4, 64) * p.table_size_mult);
     B.table.alloc(B.table_size); B.cstart.alloc(B.table_size); B.cend.alloc(B.table_size);
     B.mask.alloc(n * static_cast<size_t>(B.mask_words));
+    if (n * static_cast<size_t>(B.nbr_width) >= (1ull << 32)) B.nbr_width = 0;   // 32-bit list slot indices
+    B.nbr.alloc(n * static_cast<size_t>(B.nbr_width));
+    B.nbr_cnt.alloc(n);
     B.rho.alloc(n); B.prs.alloc(n); B.xq.alloc(n); B.vq.alloc(n); B.xr.alloc(n); B.ap.alloc(n); B.normal.alloc(n); B.vlap.alloc(n); B.anp.alloc(n);
     B.partials.alloc(2ull * pass_max_warps(B.n));
     B.group_done.alloc(pass_max_warps(B.n) / 32u + 1u);

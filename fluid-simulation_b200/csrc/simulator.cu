@@ -186,6 +186,12 @@ void CUDASPHSimulator::ensure_tables() {
     }
     const size_t words = static_cast<size_t>(n_) * static_cast<size_t>(cfg_.mask_words);
     if (mask_.count != words) mask_.alloc(words);
+    const size_t slots = static_cast<size_t>(n_) * static_cast<size_t>(cfg_.nbr_width);
+    if (slots >= (1ull << 32))   // list slots are addressed with 32-bit indices
+        throw Error(WCSPH_ERR_CONFIG, "neighbour_list_width * particles must stay below 2^32 (use a smaller width or 0)");
+    if (nbr_.count != slots) nbr_.alloc(slots);
+    const size_t counts = cfg_.nbr_width > 0 ? n_ : 0;
+    if (nbr_cnt_.count != counts) nbr_cnt_.alloc(counts);
 }
 
 // Boundary: Morton-sort once, hash (cell = h) and Akinci masses
@@ -265,6 +271,9 @@ TravArgs CUDASPHSimulator::trav_args(float delta) {
     a.mask = mask_.ptr;
     a.mask_words = static_cast<u32>(cfg_.mask_words);
     a.chunk = effective_chunk(cfg_, n_);
+    a.nbr = cfg_.nbr_width > 0 ? nbr_.ptr : nullptr;
+    a.nbr_cnt = nbr_cnt_.ptr;
+    a.nbr_width = static_cast<u32>(cfg_.nbr_width);
     a.rho = rho_.ptr; a.prs = prs_.ptr;
     a.xq = xq_.ptr; a.vq = vq_.ptr; a.xr = xr_.ptr;
     a.ap = ap_.ptr; a.normal = normal_.ptr; a.vlap = vlap_.ptr; a.anp = anp_.ptr;
@@ -442,6 +451,8 @@ void CUDASPHSimulator::apply_config(const StepConfig& c) {
     if (c.mask_words < 1 || c.mask_words > 16) throw Error(WCSPH_ERR_CONFIG, "mask_words must be in [1, 16]");
     if (c.chunk != 0 && c.chunk != 8 && c.chunk != 16 && c.chunk != 32)
         throw Error(WCSPH_ERR_CONFIG, "particles_per_warp must be 8, 16 or 32");
+    if (c.nbr_width < 0 || c.nbr_width > 1024)
+        throw Error(WCSPH_ERR_CONFIG, "neighbour_list_width must be in [0, 1024]");
     cfg_ = c;
     params_.cell_size_mult = c.cell_size_mult;
     params_.table_size_mult = c.table_size_mult;

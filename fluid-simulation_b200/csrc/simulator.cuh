@@ -76,6 +76,7 @@ struct StepConfig {
     int warps_surface = 2;
     int mask_words = 10;        // neighbour bit-matrix words per particle (cap = 32*words)
     int chunk = 0;              // sorted particles per warp: 8, 16, 32; 0 = by scene size
+    int nbr_width = 64;         // neighbour-list slots per particle; 0 = walk the bit matrix
     float cell_size_mult = 1.f;
     uint32_t table_size_mult = 1;
     bool operator==(const StepConfig&) const = default;
@@ -189,6 +190,7 @@ private:
     DevBuf<u32> cstart_, cend_;
     uint32_t table_size_ = 0;
     DevBuf<u32> mask_;
+    DevBuf<u32> nbr_, nbr_cnt_;  // neighbour lists (cfg_.nbr_width slots per particle) and counts
     DevBuf<float> rho_, prs_;
     DevBuf<float4> xq_, vq_, xr_;
     DevBuf<u64> ckeys_;         // order-equivalent short sort keys (radix_sort.cuh)

@@ -31,7 +31,9 @@ __device__ __forceinline__ u32 warp_incl_scan(u32 v) {
 //   DENSITY: positions in blocks of 16 candidate pairs, each pair as
 //            (x0,x1)(y0,y1)(z0,z1) float2s, one pad float2 per block (so that
 //            lanes on different blocks hit different banks); the distance
-//            test reads a pair per packed FP32 step
+//            test reads a pair per packed FP32 step; the range (cell) of
+//            each candidate as a byte, from which its neighbour-list entry
+//            rstart[q] + m - rpref[q] follows
 //   COUNT / FILL / ADJ_*: float4 positions and particle indices
 //   FORCE / SURFACE: particle indices only (they visit neighbours only and
 //            read the neighbour's fields through L1)
@@ -41,6 +43,7 @@ struct KindCfg {
     static constexpr bool stage_sa =
         KIND == PASS_COUNT || KIND == PASS_FILL || KIND == PASS_ADJ_FORCE || KIND == PASS_ADJ_DENSITY;
     static constexpr bool stage_j = KIND != PASS_DENSITY;
+    static constexpr bool stage_q = KIND == PASS_DENSITY;   // the candidate's range (neighbour lists)
     static constexpr bool boundary =
         KIND == PASS_DENSITY || KIND == PASS_FORCE || KIND == PASS_ADJ_FORCE || KIND == PASS_ADJ_DENSITY;
     static constexpr int nf = (KIND == PASS_FORCE || KIND == PASS_ADJ_FORCE) ? 9
@@ -64,6 +67,7 @@ struct WarpView {
     float4* sa;
     float2* sp;    // density: candidate pair positions (pair_slot layout)
     u32* cand;
+    unsigned char* cq;   // density: range of each candidate
     u32* rstart;   // fluid cells: first particle
     u32* rpref;    // fluid cells: exclusive prefix of the cell sizes (+ total)
     u32* bcand;
@@ -74,9 +78,10 @@ struct WarpView {
     u32* hoff;     // row hit offsets (HOME_BLOCK + 1)
 };
 
+// ncell = (2R + 1)^3 fluid neighbour cells.
 template <int KIND>
-__host__ __device__ __forceinline__ size_t warp_smem_bytes(u32 cap, bool with_boundary, WarpView<KIND>* v = nullptr,
-                                                           unsigned char* base = nullptr) {
+__host__ __device__ __forceinline__ size_t warp_smem_bytes(u32 cap, u32 ncell, bool with_boundary,
+                                                           WarpView<KIND>* v = nullptr, unsigned char* base = nullptr) {
     using C = KindCfg<KIND>;
     size_t o = 0;
     auto take = [&](size_t bytes) {
@@ -87,8 +92,9 @@ __host__ __device__ __forceinline__ size_t warp_smem_bytes(u32 cap, bool with_bo
     unsigned char* sa = C::stage_sa ? take(16ull * cap) : nullptr;
     unsigned char* sp = C::soa ? take(8ull * pair_slot(cap / 2)) : nullptr;
     unsigned char* cand = C::stage_j ? take(4ull * cap) : nullptr;
-    unsigned char* rstart = take(4ull * (MAX_RANGE_CELLS + 3));
-    unsigned char* rpref = take(4ull * (MAX_RANGE_CELLS + 3));
+    unsigned char* cq = C::stage_q ? take(cap) : nullptr;
+    unsigned char* rstart = take(4ull * (ncell + 3));
+    unsigned char* rpref = take(4ull * (ncell + 3));
     unsigned char *bcand = nullptr, *bstart = nullptr, *bpref = nullptr;
     if (C::boundary && with_boundary) {   // only scenes with boundary particles
         bcand = take(4ull * BCAND_CAP);
@@ -103,6 +109,7 @@ __host__ __device__ __forceinline__ size_t warp_smem_bytes(u32 cap, bool with_bo
         v->sa = reinterpret_cast<float4*>(sa);
         v->sp = reinterpret_cast<float2*>(sp);
         v->cand = reinterpret_cast<u32*>(cand);
+        v->cq = cq;
         v->rstart = reinterpret_cast<u32*>(rstart);
         v->rpref = reinterpret_cast<u32*>(rpref);
         v->bcand = reinterpret_cast<u32*>(bcand);
@@ -197,6 +204,7 @@ __device__ __forceinline__ void stage(const WarpView<KIND>& S, const TravArgs& a
             const u32 j = src + t;
             const u32 ml = lo + t - c0;
             if constexpr (KindCfg<KIND>::stage_j) S.cand[ml] = j;
+            if constexpr (KindCfg<KIND>::stage_q) S.cq[ml] = static_cast<unsigned char>(q);
             if constexpr (KindCfg<KIND>::stage_sa) S.sa[ml] = __ldg(a.pos + j);
             if constexpr (KindCfg<KIND>::soa) soa_store(S, ml, __ldg(a.pos + j));
         }
@@ -218,22 +226,30 @@ struct Nbr {
     u32 j;
 };
 
+// Neighbour records of particle j (force and surface passes).
+template <int KIND>
+__device__ __forceinline__ Nbr fetch_j(const TravArgs& a, u32 j) {
+    Nbr d;
+    d.j = j;
+    if constexpr (KIND == PASS_FORCE) {
+        d.x = __ldg(a.xq + j);
+        d.b = __ldg(a.vq + j);
+    } else {
+        d.x = __ldg(a.xr + j);
+        d.b = __ldg(a.normal + j);
+    }
+    d.c = d.x.w;
+    return d;
+}
+
 template <int KIND>
 __device__ __forceinline__ Nbr fetch(const WarpView<KIND>& S, const TravArgs& a, u32 m) {
     Nbr d;
     if constexpr (KindCfg<KIND>::soa) {
         const float* f = reinterpret_cast<const float*>(S.sp + pair_slot(m >> 1)) + (m & 1u);
         d.x = make_float4(f[0], f[2], f[4], 0.f);
-    } else if constexpr (KIND == PASS_FORCE) {
-        d.j = S.cand[m];
-        d.x = __ldg(a.xq + d.j);
-        d.b = __ldg(a.vq + d.j);
-        d.c = d.x.w;
-    } else if constexpr (KIND == PASS_SURFACE) {
-        d.j = S.cand[m];
-        d.x = __ldg(a.xr + d.j);
-        d.b = __ldg(a.normal + d.j);
-        d.c = d.x.w;
+    } else if constexpr (KIND == PASS_FORCE || KIND == PASS_SURFACE) {
+        d = fetch_j<KIND>(a, S.cand[m]);
     } else {
         d.j = S.cand[m];
         d.x = S.sa[m];
@@ -481,10 +497,11 @@ __device__ __forceinline__ void store_partial(float* part, u32 slot, const float
     for (int f = 0; f < NF; ++f) part[slot * NF + f] = v[f];
 }
 
-// Row k = lane owns items [lo, hi); c = run length.
+// Row k (the calling lane's row, lane - first row of the run) owns items
+// [lo, hi); c = run length.
 template <int NF>
-__device__ __forceinline__ void combine(const float* part, float* res, bool active, u32 lo, u32 hi, u32 c) {
-    const u32 k = lane_id();
+__device__ __forceinline__ void combine(const float* part, float* res, bool active, u32 lo, u32 hi, u32 c,
+                                        u32 k) {
     if (active && hi > lo) {
         const u32 l_lo = lo / c, l_hi = (hi - 1) / c;
         for (u32 l = l_lo; l <= l_hi; ++l) {
@@ -540,10 +557,12 @@ __device__ __forceinline__ u32 fluid_pair_run(const WarpView<KIND>& S, const Dev
 // Neighbour pairs of rows [0, nh) read from the block's bit matrix in
 // global memory (bits, row length M), split by hits. Returns the run length
 // (0: no hits) and, for row k = lane, its hit range [lo, hi).
+// lists (density pass): hit r of row k also goes to slot r of particle
+// i0 + k, nbr[r * n + i0 + k], for r < nbr_width.
 template <int KIND, bool SHARED_BITS = false>
 __device__ __forceinline__ u32 fluid_hit_run(const WarpView<KIND>& S, const DevParams& P, const TravArgs& a,
                                              const u32* __restrict__ bits, u32 nh, u32 M, u32 i0, u32& lo,
-                                             u32& hi) {
+                                             u32& hi, bool lists = false) {
     auto ld = [&](u32 w) -> u32 {
         if constexpr (SHARED_BITS) return bits[w];
         else return __ldg(bits + w);
@@ -595,6 +614,9 @@ __device__ __forceinline__ u32 fluid_hit_run(const WarpView<KIND>& S, const DevP
         float v[NF];
 #pragma unroll
         for (int f = 0; f < NF; ++f) v[f] = 0.f;
+        // density lists: list slot of hit h is h - (first hit of its row); u32
+        // indices (n * nbr_width < 2^32 is checked on the host)
+        u32 slot_base = hoff[k];
         while (word) {
             const u32 b = __ffs(word) - 1;
             word &= word - 1;
@@ -605,6 +627,15 @@ __device__ __forceinline__ u32 fluid_hit_run(const WarpView<KIND>& S, const DevP
                 for (int f = 0; f < NF; ++f) v[f] = 0.f;
                 do { ++k; row0 += M; } while (p >= row0 + M);
                 H = load_home<KIND>(a, i0 + k);
+                slot_base = hoff[k];
+            }
+            if constexpr (KIND == PASS_DENSITY) {
+                const u32 slot = h - slot_base;
+                if (lists && slot < a.nbr_width) {
+                    const u32 m = p - row0;
+                    const u32 q = S.cq[m];
+                    a.nbr[slot * a.n + i0 + k] = S.rstart[q] + (m - S.rpref[q]);
+                }
             }
             const Nbr d = fetch<KIND>(S, a, p - row0);
             fluid_pair<KIND>(v, H, d, dist2(H.x, d.x), P, a);
@@ -685,6 +716,309 @@ __device__ __forceinline__ u32 boundary_pair_run(const WarpView<KIND>& S, const 
     return c;
 }
 
+// Per-row epilogue of a pass: the sums res (fluid) and resb (boundary) of
+// particle i become its fields; the surface pass integrates and adds to
+// the warp's CFL / metric reductions.
+template <int KIND, bool BATCH>
+__device__ __forceinline__ void finish_row(const DevParams& P, const TravArgs& a, u32 i, const float* res,
+                                           const float* resb, u32 row_cnt, u32 scene, float dt, float np_dt,
+                                           float& red_max, float& red_speed, float& red_speed2) {
+    if constexpr (KIND == PASS_DENSITY) {
+        // compute_density: (W(0) + sum W) * m, then + sum m_b W
+        const float rho = (P.w0 + P.cubic_factor * res[0]) * P.mass + P.cubic_factor * resb[0];
+        const float prs = tait_pressure(rho, P);
+        a.rho[i] = rho;
+        a.prs[i] = prs;
+        if (a.nbr) a.nbr_cnt[i] = row_cnt;
+        // the force pass's neighbour records
+        const float4 xi = a.pos[i];
+        const float4 vi = a.vel[i];
+        a.xq[i] = make_float4(xi.x, xi.y, xi.z, prs / (rho * rho));
+        a.vq[i] = make_float4(vi.x, vi.y, vi.z, 1.f / rho);
+    } else if constexpr (KIND == PASS_FORCE) {
+        // compute_pressure_accel_n_normal_with_boundary: m * sum_fluid, then
+        // the boundary term (compute_pressure_accel_n_normal.cu:346-364)
+        a.ap[i] = f4(P.mass * res[0] + resb[0], P.mass * res[1] + resb[1],
+                     P.mass * res[2] + resb[2]);
+        const float sn = P.h * P.mass;
+        a.normal[i] = f4(sn * res[3], sn * res[4], sn * res[5]);
+        a.vlap[i] = f4(res[6], res[7], res[8]);
+        // the surface pass's neighbour record
+        const float4 xi = a.pos[i];
+        a.xr[i] = make_float4(xi.x, xi.y, xi.z, a.rho[i]);
+    } else if constexpr (KIND == PASS_SURFACE) {
+        // a_np = g + F_ext + nu*10*m*vlap - alpha*2*rho0*f
+        const float4 xi = a.pos[i];
+        const float4 vi = a.vel[i];
+        const float4 api = a.ap[i];
+        const float4 vli = a.vlap[i];
+        const float4 fe = external_force(xi, P);
+        float4 gv = make_float4(P.gravity[0], P.gravity[1], P.gravity[2], P.visc_scale);
+        const DevBox* bb = a.box;
+        if constexpr (BATCH) {
+            gv = a.scenes[scene].gravity_visc;
+            bb = &a.scenes[scene].box;
+            a.scene_state[i] = scene;
+        }
+        float4 anp;
+        anp.x = gv.x + fe.x + gv.w * vli.x - P.st_scale * res[0];
+        anp.y = gv.y + fe.y + gv.w * vli.y - P.st_scale * res[1];
+        anp.z = gv.z + fe.z + gv.w * vli.z - P.st_scale * res[2];
+        anp.w = 0.f;
+        a.anp[i] = anp;
+        // update_positions.cu:64-67
+        float4 v = vi, x = xi;
+        v.x += np_dt * anp.x + dt * api.x;
+        v.y += np_dt * anp.y + dt * api.y;
+        v.z += np_dt * anp.z + dt * api.z;
+        x.x += dt * v.x;
+        x.y += dt * v.y;
+        x.z += dt * v.z;
+        x.w += dt * v.w;
+        resolve_collision(x, v, *bb, P);
+        a.pos_out[i] = x;
+        a.vel_out[i] = v;
+        const float s2 = dot3(v, v);
+        red_max = fmaxf(red_max, s2);
+        red_speed += sqrtf(s2);
+        red_speed2 += s2;
+    } else if constexpr (KIND == PASS_ADJ_FORCE) {
+        const float rho_i = a.rho[i];
+        const float prs_i = a.prs[i];
+        const float pt = res[6], vt = res[7], bt = resb[3];
+        const float inv_r2 = 1.f / (rho_i * rho_i);
+        const float pbar = pt * inv_r2 + bt * (inv_r2 + 1.f / P.rest_density2);
+        float rhobar = (pt + bt) * (-2.f * prs_i * inv_r2 / rho_i) + vt * inv_r2;
+        // Tait EOS with the clamp of compute_rho_p.cu:236-238
+        const float ratio = rho_i / P.rest_density;
+        const float rc = fminf(fmaxf(ratio, 1.f), P.max_density_ratio);
+        if (ratio > 1.f && ratio < P.max_density_ratio)
+            rhobar += pbar * P.stiffness * P.exponent * powf(ratio, P.exponent - 1.f) / P.rest_density;
+        red_speed += pbar * (powf(rc, P.exponent) - 1.f);  // dL/dk partial
+        a.adj_rhobar[i] = rhobar;
+        const float4 xb0 = a.adj_xbar[i], vb0 = a.adj_vbar[i];
+        a.adj_xbar[i] = f4(xb0.x + res[0] + resb[0], xb0.y + res[1] + resb[1],
+                           xb0.z + res[2] + resb[2]);
+        a.adj_vbar[i] = f4(vb0.x + res[3], vb0.y + res[4], vb0.z + res[5]);
+    } else if constexpr (KIND == PASS_ADJ_DENSITY) {
+        const float4 xb0 = a.adj_xbar[i];
+        a.adj_xbar[i] = f4(xb0.x + res[0] + resb[0], xb0.y + res[1] + resb[1],
+                           xb0.z + res[2] + resb[2]);
+    }
+}
+
+// Cell coordinates (and scene) of a packed cell key.
+template <bool BATCH>
+__device__ __forceinline__ void decode_cell(u64 pk, u32& ux, u32& uy, u32& uz, u32& scene) {
+    if constexpr (BATCH) {
+        scene = static_cast<u32>(pk >> 48);
+        ux = static_cast<u32>(pk & 0xFFFFull);
+        uy = static_cast<u32>((pk >> 16) & 0xFFFFull);
+        uz = static_cast<u32>((pk >> 32) & 0xFFFFull);
+    } else {
+        scene = 0;
+        ux = static_cast<u32>(pk & 0x1FFFFFull);
+        uy = static_cast<u32>((pk >> 21) & 0x1FFFFFull);
+        uz = static_cast<u32>((pk >> 42) & 0x1FFFFFull);
+    }
+}
+
+// The fluid sums of one row (particle i) without its list: lane q walks
+// neighbour cells q, q + 32, ... of i's cell (its hash probe and particles),
+// testing every candidate against h^2; the lanes' partials are then added
+// in a fixed butterfly order. Returns the sums on every lane.
+template <int KIND, bool BATCH>
+__device__ __forceinline__ void spill_row(const DevParams& P, const TravArgs& a, u32 i, float* out) {
+    constexpr int NF = KindCfg<KIND>::nf;
+    const u32 lane = lane_id();
+    u32 ux, uy, uz, scene;
+    decode_cell<BATCH>(a.ckey[i], ux, uy, uz, scene);
+    const int R = a.range;
+    const u32 D = static_cast<u32>(2 * R + 1);
+    const u32 ncell = D * D * D;
+    const HomeData H = load_home<KIND>(a, i);
+    float v[NF];
+#pragma unroll
+    for (int f = 0; f < NF; ++f) v[f] = 0.f;
+    for (u32 q = lane; q < ncell; q += 32) {
+        const int dz = static_cast<int>(q % D) - R;
+        const int dy = static_cast<int>((q / D) % D) - R;
+        const int dx = static_cast<int>(q / (D * D)) - R;
+        u64 pk;
+        if constexpr (BATCH) pk = pack_cell_batch(scene, ux + dx, uy + dy, uz + dz);
+        else pk = pack_cell(ux + dx, uy + dy, uz + dz);
+        const u32 slot = hash_find<BATCH>(a.fluid.table, a.fluid.tmask, pk);
+        if (slot == EMPTY_CELL) continue;
+        const u32 e = __ldg(a.fluid.cend + slot);
+        for (u32 j = __ldg(a.fluid.cstart + slot); j < e; ++j) {
+            const Nbr d = fetch_j<KIND>(a, j);
+            const float r2 = dist2(H.x, d.x);
+            if (r2 <= P.h2 && j != i) fluid_pair<KIND>(v, H, d, r2, P, a);
+        }
+    }
+#pragma unroll
+    for (int f = 0; f < NF; ++f) {
+        float x = v[f];
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(FULL, x, o);
+        out[f] = x;
+    }
+}
+
+// Boundary sums of one row (particle i, home data H): the 3x3x3 boundary
+// cells around its own cell in x, y, z nesting order, as for_boundary_neighbors
+// (common.cuh:153-178) visits them, one particle after the other.
+template <int KIND, bool BATCH>
+__device__ __forceinline__ void boundary_row(const DevParams& P, const TravArgs& a, const HomeData& H, u32 scene,
+                                             float* resb) {
+    const int3 c = cell_of(H.x, P.h);
+    for (int dx = -1; dx <= 1; ++dx)
+        for (int dy = -1; dy <= 1; ++dy)
+            for (int dz = -1; dz <= 1; ++dz) {
+                u64 pk;
+                if constexpr (BATCH)
+                    pk = pack_cell_batch(scene, offset_coord(c.x + dx), offset_coord(c.y + dy), offset_coord(c.z + dz));
+                else pk = pack_cell(make_int3(c.x + dx, c.y + dy, c.z + dz));
+                const u32 slot = hash_find<BATCH>(a.boundary.table, a.boundary.tmask, pk);
+                if (slot == EMPTY_CELL) continue;
+                const u32 e = __ldg(a.boundary.cend + slot);
+                for (u32 b = __ldg(a.boundary.cstart + slot); b < e; ++b) {
+                    const float4 xb = __ldg(a.bpos + b);
+                    const float r2 = dist2(H.x, xb);
+                    if (r2 <= P.h2) boundary_pair<KIND>(resb, H, b, xb, r2, P, a);
+                }
+            }
+}
+
+// Force / surface pass over listed neighbours: the warp's rows are the
+// particles [i0, i0 + nh) of its chunk, whatever their cells; lane k sums
+// row k's list in order (the reference's per-particle order), so a row's
+// sums do not depend on which particles share its warp.
+template <int KIND, bool BATCH>
+__device__ __forceinline__ void list_rows(const DevParams& P, const TravArgs& a, u32 i0, u32 nh, float dt,
+                                          float np_dt, float& red_max, float& red_speed, float& red_speed2) {
+    using C = KindCfg<KIND>;
+    constexpr int NF = C::nf;
+    constexpr int NFB = C::nfb;
+    const u32 lane = lane_id();
+    const bool act = lane < nh;
+    const u32 i = i0 + (act ? lane : 0u);
+    const u32 cnt = act ? __ldg(a.nbr_cnt + i) : 0u;
+    const bool spill = act && cnt > a.nbr_width;
+    float res[NF], resb[NFB];
+#pragma unroll
+    for (int f = 0; f < NF; ++f) res[f] = 0.f;
+    for (u32 sp = __ballot_sync(FULL, spill); sp; sp &= sp - 1) {
+        const u32 f = __ffs(sp) - 1;
+        float t[NF];
+        spill_row<KIND, BATCH>(P, a, i0 + f, t);
+        if (lane == f) {
+#pragma unroll
+            for (int g = 0; g < NF; ++g) res[g] = t[g];
+        }
+    }
+#pragma unroll
+    for (int f = 0; f < NFB; ++f) resb[f] = 0.f;
+    const u64 pk = act ? a.ckey[i] : 0ull;
+    const u32 scene = BATCH ? static_cast<u32>(pk >> 48) : 0u;
+    if (act) {
+        const HomeData H = load_home<KIND>(a, i);
+        if (!spill && cnt > 0) {
+            // slot t of row i at nbr[t * n + i]; the next neighbour's records
+            // and the index after it are in flight while a pair is summed
+            const size_t stride = a.n;
+            const u32* lst = a.nbr + i + stride;
+            Nbr d = fetch_j<KIND>(a, __ldg(a.nbr + i));
+            u32 jn = cnt > 1 ? __ldg(lst) : 0u;
+            lst += stride;
+            for (u32 t = 0; t < cnt; ++t) {
+                Nbr dn = d;
+                if (t + 1 < cnt) dn = fetch_j<KIND>(a, jn);
+                if (t + 2 < cnt) {
+                    jn = __ldg(lst);
+                    lst += stride;
+                }
+                fluid_pair<KIND>(res, H, d, dist2(H.x, d.x), P, a);
+                d = dn;
+            }
+        }
+        if constexpr (C::boundary) {
+            if (a.nb > 0) boundary_row<KIND, BATCH>(P, a, H, scene, resb);
+        }
+    }
+    if (act) finish_row<KIND, BATCH>(P, a, i, res, resb, 0u, scene, dt, np_dt, red_max, red_speed, red_speed2);
+}
+
+// Surface pass: CFL max |v|^2 and the metric sums without block barriers:
+// warp partials -> groups of 32 warps -> whole grid; each level is finished
+// by its last arriving warp and summed in index order (deterministic). The
+// last warp also publishes dt and flips the max-speed parity.
+template <int WPB>
+__device__ __forceinline__ void surface_reduce(const TravArgs& a, float dt, float np_dt, float red_max, float red_speed,
+                                               float red_speed2) {
+    const u32 lane = lane_id();
+    const u32 warp = threadIdx.x >> 5;
+    const u32 n = a.n;
+    for (int o = 16; o > 0; o >>= 1) {
+        red_max = fmaxf(red_max, __shfl_xor_sync(FULL, red_max, o));
+        red_speed += __shfl_xor_sync(FULL, red_speed, o);
+        red_speed2 += __shfl_xor_sync(FULL, red_speed2, o);
+    }
+    const u32 nwarps = gridDim.x * WPB;
+    const u32 gw = blockIdx.x * WPB + warp;
+    const u32 group = gw >> 5;
+    const u32 ngroups = (nwarps + 31u) >> 5;
+    const u32 gsize = min(32u, nwarps - (group << 5));
+    u32 last = 0;
+    if (lane == 0) {
+        a.block_partials[2 * gw] = red_speed;
+        a.block_partials[2 * gw + 1] = red_speed2;
+        atomicMax(&a.st->vmax2_bits[a.st->parity ^ 1u], __float_as_uint(red_max));
+        __threadfence();
+        last = atomicAdd(a.group_done + group, 1u) == gsize - 1 ? 1u : 0u;
+    }
+    if (__shfl_sync(FULL, last, 0)) {
+        __threadfence();
+        const u32 w = (group << 5) + lane;
+        double s1 = lane < gsize ? static_cast<double>(__ldcg(a.block_partials + 2 * w)) : 0.0;
+        double s2 = lane < gsize ? static_cast<double>(__ldcg(a.block_partials + 2 * w + 1)) : 0.0;
+        for (int o = 16; o > 0; o >>= 1) {
+            s1 += __shfl_xor_sync(FULL, s1, o);
+            s2 += __shfl_xor_sync(FULL, s2, o);
+        }
+        u32 top = 0;
+        if (lane == 0) {
+            a.group_partials[2 * group] = s1;
+            a.group_partials[2 * group + 1] = s2;
+            a.group_done[group] = 0u;
+            __threadfence();
+            top = atomicAdd(&a.st->blocks_done, 1u) == ngroups - 1 ? 1u : 0u;
+        }
+        if (__shfl_sync(FULL, top, 0)) {
+            __threadfence();
+            double t1 = 0.0, t2 = 0.0;
+            for (u32 g = lane; g < ngroups; g += 32) {
+                t1 += __ldcg(a.group_partials + 2 * g);
+                t2 += __ldcg(a.group_partials + 2 * g + 1);
+            }
+            for (int o = 16; o > 0; o >>= 1) {
+                t1 += __shfl_xor_sync(FULL, t1, o);
+                t2 += __shfl_xor_sync(FULL, t2, o);
+            }
+            if (lane == 0) {
+                DevState* st = a.st;
+                st->last_mean_speed = static_cast<float>(t1 / static_cast<double>(n));
+                st->last_ke = static_cast<float>(0.5 * static_cast<double>(a.metric_mass) * t2);
+                st->last_dt_p = dt;
+                st->last_np_dt = np_dt;
+                const u32 old = st->parity;
+                st->vmax2_bits[old] = 0u;
+                st->parity = old ^ 1u;
+                st->blocks_done = 0u;
+            }
+        }
+    }
+}
+
 template <int KIND, int WPB, bool BATCH>
 __global__ void __launch_bounds__(WPB * 32, KindCfg<KIND>::min_warps / WPB) cell_pass_kernel(const DevParams P, const TravArgs a) {
     using C = KindCfg<KIND>;
@@ -696,8 +1030,9 @@ __global__ void __launch_bounds__(WPB * 32, KindCfg<KIND>::min_warps / WPB) cell
     const u32 cap = a.mask_words * 32u;
     WarpView<KIND> S;
     const bool with_boundary = a.nb > 0;
-    const size_t wbytes = warp_smem_bytes<KIND>(cap, with_boundary);
-    warp_smem_bytes<KIND>(cap, with_boundary, &S, dyn_smem + warp * wbytes);
+    const u32 ncell_s = static_cast<u32>((2 * a.range + 1) * (2 * a.range + 1) * (2 * a.range + 1));
+    const size_t wbytes = warp_smem_bytes<KIND>(cap, ncell_s, with_boundary);
+    warp_smem_bytes<KIND>(cap, ncell_s, with_boundary, &S, dyn_smem + warp * wbytes);
 
     float dt = 0.f, np_dt = 0.f;
     if constexpr (KIND == PASS_SURFACE) {
@@ -808,6 +1143,7 @@ __global__ void __launch_bounds__(WPB * 32, KindCfg<KIND>::min_warps / WPB) cell
                 for (int f = 0; f < NF; ++f) res[f] = 0.f;
 #pragma unroll
                 for (int f = 0; f < NFB; ++f) resb[f] = 0.f;
+                u32 row_cnt = NBR_SPILL;   // density with lists: the row's listed neighbour count
 
                 if constexpr (KIND == PASS_COUNT || KIND == PASS_FILL) {
                     // sequential per home particle, in candidate order (the reference's order)
@@ -857,7 +1193,8 @@ __global__ void __launch_bounds__(WPB * 32, KindCfg<KIND>::min_warps / WPB) cell
                     continue;
                 } else if constexpr (KIND == PASS_DENSITY) {
                     // phase 1 tests every candidate and builds the bit matrix in shared
-                    // memory; phase 2 sums W over the neighbours only
+                    // memory; phase 2 sums W over the neighbours only (and, with
+                    // lists on, writes them to the rows' lists)
                     auto density_chunk = [&](u32 c0, u32 len, bool keep_bits) {
                         const u32 wpr = (len + 31u) >> 5;
                         const u32 len32 = wpr << 5;
@@ -870,8 +1207,10 @@ __global__ void __launch_bounds__(WPB * 32, KindCfg<KIND>::min_warps / WPB) cell
                         }
                         __syncwarp();
                         u32 lo, hi;
-                        const u32 c = fluid_hit_run<KIND, true>(S, P, a, S.aux, nh, len32, i0, lo, hi);
-                        if (c) combine<NF>(S.part, res, act, lo, hi, c);
+                        const u32 c = fluid_hit_run<KIND, true>(S, P, a, S.aux, nh, len32, i0, lo, hi,
+                                                                keep_bits && a.nbr != nullptr);
+                        if (c) combine<NF>(S.part, res, act, lo, hi, c, lane);
+                        if (keep_bits && hi - lo <= a.nbr_width) row_cnt = hi - lo;
                         if (keep_bits)
                             for (u32 w = lane; w < nwords; w += 32) blk_bits[w] = S.aux[w];
                         __syncwarp();
@@ -893,13 +1232,13 @@ __global__ void __launch_bounds__(WPB * 32, KindCfg<KIND>::min_warps / WPB) cell
                         __syncwarp();
                         u32 lo, hi;
                         const u32 c = fluid_hit_run<KIND, true>(S, P, a, S.aux, nh, Mrow, i0, lo, hi);
-                        if (c) combine<NF>(S.part, res, act, lo, hi, c);
+                        if (c) combine<NF>(S.part, res, act, lo, hi, c, lane);
                     } else {
                         for (u32 c0 = 0; c0 < M; c0 += cap) {
                             const u32 len = min(cap, M - c0);
                             stage<KIND>(S, a, ncell, c0, len);
                             const u32 c = fluid_pair_run<KIND>(S, P, a, nh, len, c0, i0, self0);
-                            combine<NF>(S.part, res, act, lane * len, lane * len + len, c);
+                            combine<NF>(S.part, res, act, lane * len, lane * len + len, c, lane);
                         }
                     }
                 }
@@ -910,93 +1249,13 @@ __global__ void __launch_bounds__(WPB * 32, KindCfg<KIND>::min_warps / WPB) cell
                         const u32 len = min(BCAND_CAP, MB - c0);
                         expand(S.bcand, S.bstart, S.bpref, nbc, c0, len);
                         const u32 c = boundary_pair_run<KIND>(S, P, a, nh, len, i0);
-                        combine<NFB>(S.part, resb, act, lane * len, lane * len + len, c);
+                        combine<NFB>(S.part, resb, act, lane * len, lane * len + len, c, lane);
                     }
                 }
 
-                if (act) {
-                    if constexpr (KIND == PASS_DENSITY) {
-                        // compute_density: (W(0) + sum W) * m, then + sum m_b W
-                        const float rho = (P.w0 + P.cubic_factor * res[0]) * P.mass + P.cubic_factor * resb[0];
-                        const float prs = tait_pressure(rho, P);
-                        a.rho[i] = rho;
-                        a.prs[i] = prs;
-                        // the force pass's neighbour records
-                        const float4 xi = a.pos[i];
-                        const float4 vi = a.vel[i];
-                        a.xq[i] = make_float4(xi.x, xi.y, xi.z, prs / (rho * rho));
-                        a.vq[i] = make_float4(vi.x, vi.y, vi.z, 1.f / rho);
-                    } else if constexpr (KIND == PASS_FORCE) {
-                        // compute_pressure_accel_n_normal_with_boundary: m * sum_fluid, then
-                        // the boundary term (compute_pressure_accel_n_normal.cu:346-364)
-                        a.ap[i] = f4(P.mass * res[0] + resb[0], P.mass * res[1] + resb[1],
-                                     P.mass * res[2] + resb[2]);
-                        const float sn = P.h * P.mass;
-                        a.normal[i] = f4(sn * res[3], sn * res[4], sn * res[5]);
-                        a.vlap[i] = f4(res[6], res[7], res[8]);
-                        // the surface pass's neighbour record
-                        const float4 xi = a.pos[i];
-                        a.xr[i] = make_float4(xi.x, xi.y, xi.z, a.rho[i]);
-                    } else if constexpr (KIND == PASS_SURFACE) {
-                        // a_np = g + F_ext + nu*10*m*vlap - alpha*2*rho0*f
-                        const float4 xi = a.pos[i];
-                        const float4 vi = a.vel[i];
-                        const float4 api = a.ap[i];
-                        const float4 vli = a.vlap[i];
-                        const float4 fe = external_force(xi, P);
-                        float4 gv = make_float4(P.gravity[0], P.gravity[1], P.gravity[2], P.visc_scale);
-                        const DevBox* bb = a.box;
-                        if constexpr (BATCH) {
-                            gv = a.scenes[scene].gravity_visc;
-                            bb = &a.scenes[scene].box;
-                            a.scene_state[i] = scene;
-                        }
-                        float4 anp;
-                        anp.x = gv.x + fe.x + gv.w * vli.x - P.st_scale * res[0];
-                        anp.y = gv.y + fe.y + gv.w * vli.y - P.st_scale * res[1];
-                        anp.z = gv.z + fe.z + gv.w * vli.z - P.st_scale * res[2];
-                        anp.w = 0.f;
-                        a.anp[i] = anp;
-                        // update_positions.cu:64-67
-                        float4 v = vi, x = xi;
-                        v.x += np_dt * anp.x + dt * api.x;
-                        v.y += np_dt * anp.y + dt * api.y;
-                        v.z += np_dt * anp.z + dt * api.z;
-                        x.x += dt * v.x;
-                        x.y += dt * v.y;
-                        x.z += dt * v.z;
-                        x.w += dt * v.w;
-                        resolve_collision(x, v, *bb, P);
-                        a.pos_out[i] = x;
-                        a.vel_out[i] = v;
-                        const float s2 = dot3(v, v);
-                        red_max = fmaxf(red_max, s2);
-                        red_speed += sqrtf(s2);
-                        red_speed2 += s2;
-                    } else if constexpr (KIND == PASS_ADJ_FORCE) {
-                        const float rho_i = a.rho[i];
-                        const float prs_i = a.prs[i];
-                        const float pt = res[6], vt = res[7], bt = resb[3];
-                        const float inv_r2 = 1.f / (rho_i * rho_i);
-                        const float pbar = pt * inv_r2 + bt * (inv_r2 + 1.f / P.rest_density2);
-                        float rhobar = (pt + bt) * (-2.f * prs_i * inv_r2 / rho_i) + vt * inv_r2;
-                        // Tait EOS with the clamp of compute_rho_p.cu:236-238
-                        const float ratio = rho_i / P.rest_density;
-                        const float rc = fminf(fmaxf(ratio, 1.f), P.max_density_ratio);
-                        if (ratio > 1.f && ratio < P.max_density_ratio)
-                            rhobar += pbar * P.stiffness * P.exponent * powf(ratio, P.exponent - 1.f) / P.rest_density;
-                        red_speed += pbar * (powf(rc, P.exponent) - 1.f);  // dL/dk partial
-                        a.adj_rhobar[i] = rhobar;
-                        const float4 xb0 = a.adj_xbar[i], vb0 = a.adj_vbar[i];
-                        a.adj_xbar[i] = f4(xb0.x + res[0] + resb[0], xb0.y + res[1] + resb[1],
-                                           xb0.z + res[2] + resb[2]);
-                        a.adj_vbar[i] = f4(vb0.x + res[3], vb0.y + res[4], vb0.z + res[5]);
-                    } else if constexpr (KIND == PASS_ADJ_DENSITY) {
-                        const float4 xb0 = a.adj_xbar[i];
-                        a.adj_xbar[i] = f4(xb0.x + res[0] + resb[0], xb0.y + res[1] + resb[1],
-                                           xb0.z + res[2] + resb[2]);
-                    }
-                }
+                if (act)
+                    finish_row<KIND, BATCH>(P, a, i, res, resb, row_cnt, scene, dt, np_dt, red_max, red_speed,
+                                            red_speed2);
             }
         }
     }
@@ -1006,70 +1265,34 @@ __global__ void __launch_bounds__(WPB * 32, KindCfg<KIND>::min_warps / WPB) cell
         for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
         if (lane == 0 && v != 0.0) atomicAdd(a.adj_accum, v);
     }
+    if constexpr (KIND == PASS_SURFACE) surface_reduce<WPB>(a, dt, np_dt, red_max, red_speed, red_speed2);
+}
+
+// Resident warps per SM the register allocation of the list kernels must
+// allow (32 -> 64 registers, 40 -> 48).
+template <int KIND>
+struct ListCfg {
+    static constexpr int min_warps = KIND == PASS_FORCE ? 32 : 40;
+};
+
+// Force / surface pass over the neighbour lists written by the density pass.
+template <int KIND, int WPB, bool BATCH>
+__global__ void __launch_bounds__(WPB * 32, ListCfg<KIND>::min_warps / WPB) list_pass_kernel(const DevParams P,
+                                                                                          const TravArgs a) {
+    const u32 lane = lane_id();
+    const u32 warp = threadIdx.x >> 5;
+    float dt = 0.f, np_dt = 0.f;
     if constexpr (KIND == PASS_SURFACE) {
-        // CFL max |v|^2 and the metric sums without block barriers: warp
-        // partials -> groups of 32 warps -> whole grid; each level is finished
-        // by its last arriving warp and summed in index order (deterministic).
-        for (int o = 16; o > 0; o >>= 1) {
-            red_max = fmaxf(red_max, __shfl_xor_sync(FULL, red_max, o));
-            red_speed += __shfl_xor_sync(FULL, red_speed, o);
-            red_speed2 += __shfl_xor_sync(FULL, red_speed2, o);
-        }
-        const u32 nwarps = gridDim.x * WPB;
-        const u32 gw = blockIdx.x * WPB + warp;
-        const u32 group = gw >> 5;
-        const u32 ngroups = (nwarps + 31u) >> 5;
-        const u32 gsize = min(32u, nwarps - (group << 5));
-        u32 last = 0;
-        if (lane == 0) {
-            a.block_partials[2 * gw] = red_speed;
-            a.block_partials[2 * gw + 1] = red_speed2;
-            atomicMax(&a.st->vmax2_bits[a.st->parity ^ 1u], __float_as_uint(red_max));
-            __threadfence();
-            last = atomicAdd(a.group_done + group, 1u) == gsize - 1 ? 1u : 0u;
-        }
-        if (__shfl_sync(FULL, last, 0)) {
-            __threadfence();
-            const u32 w = (group << 5) + lane;
-            double s1 = lane < gsize ? static_cast<double>(__ldcg(a.block_partials + 2 * w)) : 0.0;
-            double s2 = lane < gsize ? static_cast<double>(__ldcg(a.block_partials + 2 * w + 1)) : 0.0;
-            for (int o = 16; o > 0; o >>= 1) {
-                s1 += __shfl_xor_sync(FULL, s1, o);
-                s2 += __shfl_xor_sync(FULL, s2, o);
-            }
-            u32 top = 0;
-            if (lane == 0) {
-                a.group_partials[2 * group] = s1;
-                a.group_partials[2 * group + 1] = s2;
-                a.group_done[group] = 0u;
-                __threadfence();
-                top = atomicAdd(&a.st->blocks_done, 1u) == ngroups - 1 ? 1u : 0u;
-            }
-            if (__shfl_sync(FULL, top, 0)) {
-                __threadfence();
-                double t1 = 0.0, t2 = 0.0;
-                for (u32 g = lane; g < ngroups; g += 32) {
-                    t1 += __ldcg(a.group_partials + 2 * g);
-                    t2 += __ldcg(a.group_partials + 2 * g + 1);
-                }
-                for (int o = 16; o > 0; o >>= 1) {
-                    t1 += __shfl_xor_sync(FULL, t1, o);
-                    t2 += __shfl_xor_sync(FULL, t2, o);
-                }
-                if (lane == 0) {
-                    DevState* st = a.st;
-                    st->last_mean_speed = static_cast<float>(t1 / static_cast<double>(n));
-                    st->last_ke = static_cast<float>(0.5 * static_cast<double>(a.metric_mass) * t2);
-                    st->last_dt_p = dt;
-                    st->last_np_dt = np_dt;
-                    const u32 old = st->parity;
-                    st->vmax2_bits[old] = 0u;
-                    st->parity = old ^ 1u;
-                    st->blocks_done = 0u;
-                }
-            }
-        }
+        float t = 0.f;
+        if (lane == 0) t = cfl_time_step(a, P);
+        dt = __shfl_sync(FULL, t, 0);
+        np_dt = a.delta < a.np_max_dt ? a.delta : a.np_max_dt;
     }
+    float red_max = 0.f, red_speed = 0.f, red_speed2 = 0.f;
+    const u32 base = (blockIdx.x * WPB + warp) * a.chunk;
+    if (base < a.n)
+        list_rows<KIND, BATCH>(P, a, base, min(a.chunk, a.n - base), dt, np_dt, red_max, red_speed, red_speed2);
+    if constexpr (KIND == PASS_SURFACE) surface_reduce<WPB>(a, dt, np_dt, red_max, red_speed, red_speed2);
 }
 
 template <bool BATCH>
@@ -1216,11 +1439,18 @@ void launch_reorder_cells(const float4* pos_in, const float4* vel_in, const u32*
 template <int KIND, int WPB, bool BATCH>
 static void launch_wpb(const DevParams& P, const TravArgs& a, cudaStream_t stream, u32 grid) {
     // per-warp candidate staging sized by the bit-matrix capacity 32 * mask_words
-    const size_t bytes = warp_smem_bytes<KIND>(a.mask_words * 32u, a.nb > 0) * WPB;
+    if constexpr (KIND == PASS_FORCE || KIND == PASS_SURFACE) {
+        if (a.nbr) {   // the list kernels use no shared memory (all of it serves as L1)
+            list_pass_kernel<KIND, WPB, BATCH><<<grid, WPB * 32, 0, stream>>>(P, a);
+            return;
+        }
+    }
+    const u32 ncell = static_cast<u32>((2 * a.range + 1) * (2 * a.range + 1) * (2 * a.range + 1));
+    const size_t bytes = warp_smem_bytes<KIND>(a.mask_words * 32u, ncell, a.nb > 0) * WPB;
     static bool configured = false;  // per instantiation; the attribute is per device function
     if (!configured) {
         cudaFuncSetAttribute(cell_pass_kernel<KIND, WPB, BATCH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             static_cast<int>(warp_smem_bytes<KIND>(32u * MAX_MASK_WORDS, true) * WPB));
+                             static_cast<int>(warp_smem_bytes<KIND>(32u * MAX_MASK_WORDS, MAX_RANGE_CELLS, true) * WPB));
         configured = true;
     }
     cell_pass_kernel<KIND, WPB, BATCH><<<grid, WPB * 32, bytes, stream>>>(P, a);

@@ -29,9 +29,17 @@
 //                  set bits. The matrix is kept row-major in the cell's
 //                  mask_words * n_home words of the mask buffer;
 //   later passes   walk the set bits of that matrix (neighbours only).
-// The walks split the block's set bits into 32 contiguous lane runs; each
-// lane keeps one partial sum per home row it crosses and the partials are
-// added per home in lane order, so results are deterministic.
+// With neighbour lists on (nbr != nullptr), the density pass also writes each
+// particle's neighbours, in candidate order, to its nbr_width list slots
+// (slot-major, so that a warp's rows read one slot coalesced), and the force
+// and surface passes no longer look at cells: lane k of a warp takes
+// particle k of the chunk and sums its list in order, then its boundary
+// cells. Rows whose neighbours did not fit (count > nbr_width, or a cell
+// beyond the bit-matrix capacity) carry NBR_SPILL and are recomputed from
+// their cell neighbourhood by the whole warp.
+// The bit-matrix walks split the block's neighbours into 32 contiguous lane
+// runs; each lane keeps one partial sum per home row it crosses and the
+// partials are added per home in lane order, so results are deterministic.
 #pragma once
 #include "sph_common.cuh"
 
@@ -40,6 +48,7 @@ namespace wcsph {
 constexpr int MAX_RANGE_CELLS = 125;     // (2R+1)^3 with R <= 2
 constexpr int MAX_BOUNDARY_CELLS = 125;
 constexpr u32 MAX_MASK_WORDS = 16;      // bit-matrix words per particle (candidate cap = 32 * words)
+constexpr u32 NBR_SPILL = 0xFFFFFFFFu;  // neighbour count of a row whose list is not usable
 
 struct HashView {
     const u64* table;
@@ -64,6 +73,10 @@ struct TravArgs {
     u32* mask;
     u32 mask_words;           // words per particle (candidate cap = 32*mask_words)
     u32 chunk;                // sorted particles per warp chunk: 8, 16 or 32
+    // neighbour lists (nullptr: the force and surface passes walk the bit matrix)
+    u32* nbr;                 // slot t of particle i at nbr[t * n + i], t < nbr_width, candidate order
+    u32* nbr_cnt;             // per particle: neighbour count, or NBR_SPILL
+    u32 nbr_width;
     // fields
     float* rho;
     float* prs;

@@ -274,6 +274,7 @@ StepConfig Tuner::parse_config_json(const std::string& text, const StepConfig& b
         else if (e.name == "compute_non_pressure_accel_block") c.warps_surface = warps_from_block(v);
         else if (e.name == "mask_words") c.mask_words = static_cast<int>(v);
         else if (e.name == "particles_per_warp") c.chunk = static_cast<int>(v);
+        else if (e.name == "neighbour_list_width") c.nbr_width = static_cast<int>(v);
         // KTT-only parameters (KERNEL_DIR, *_u_n, *_nlist, *_shared, *_cache_log2,
         // MIN_TABLE_SIZE, EXTERNAL_FORCE ...) have no counterpart and are ignored.
     }
@@ -284,6 +285,8 @@ StepConfig Tuner::parse_config_json(const std::string& text, const StepConfig& b
     if (c.mask_words < 1 || c.mask_words > 16) throw Error(WCSPH_ERR_CONFIG, "mask_words must be in [1, 16]");
     if (c.chunk != 0 && c.chunk != 8 && c.chunk != 16 && c.chunk != 32)
         throw Error(WCSPH_ERR_CONFIG, "particles_per_warp must be 8, 16 or 32");
+    if (c.nbr_width < 0 || c.nbr_width > 1024)
+        throw Error(WCSPH_ERR_CONFIG, "neighbour_list_width must be in [0, 1024]");
     return c;
 }
 
@@ -297,10 +300,11 @@ std::string Tuner::config_json(const StepConfig& c) {
                   "  {\"Name\": \"compute_pressure_accel_n_normal_block\", \"Value\": %d, \"ValueType\": \"UnsignedInt\"},\n"
                   "  {\"Name\": \"compute_non_pressure_accel_block\", \"Value\": %d, \"ValueType\": \"UnsignedInt\"},\n"
                   "  {\"Name\": \"mask_words\", \"Value\": %d, \"ValueType\": \"UnsignedInt\"},\n"
-                  "  {\"Name\": \"particles_per_warp\", \"Value\": %d, \"ValueType\": \"UnsignedInt\"}\n"
+                  "  {\"Name\": \"particles_per_warp\", \"Value\": %d, \"ValueType\": \"UnsignedInt\"},\n"
+                  "  {\"Name\": \"neighbour_list_width\", \"Value\": %d, \"ValueType\": \"UnsignedInt\"}\n"
                   "]\n",
                   static_cast<double>(c.cell_size_mult), c.table_size_mult, c.warps_density * 32,
-                  c.warps_force * 32, c.warps_surface * 32, c.mask_words, c.chunk);
+                  c.warps_force * 32, c.warps_surface * 32, c.mask_words, c.chunk, c.nbr_width);
     return buf;
 }
 

@@ -111,8 +111,18 @@ def dam_break_scene(dims=(16, 16, 16), r=0.01, jitter_frac=0.1, seed=7, walls=Tr
     return p, bx, pos, bpos
 
 
-def run_one_step(p, bx, pos, vel, bpos, delta, **sim_kw):
+def run_one_step(p, bx, pos, vel, bpos, delta, config=None, **sim_kw):
+    """config: {name: value} entries of a frozen traversal config (KTT schema)."""
     sim = wcsph.CUDASPHSimulator(p, pos, bx, fluid_vel=vel, boundary_pos=bpos, **sim_kw)
+    if config:
+        import json, os, tempfile
+        fd, path = tempfile.mkstemp(suffix=".json")
+        with os.fdopen(fd, "w") as f:
+            json.dump([{"Name": k, "Value": v, "ValueType": "UnsignedInt"} for k, v in config.items()], f)
+        try:
+            sim.set_tuning(wcsph.SEARCH_MCMC, 0.0, path)
+        finally:
+            os.unlink(path)
     sim.update(delta)
     out = {k: sim.field(k) for k in ("position", "velocity", "density", "pressure", "pressure_accel",
                                      "non_pressure_accel", "normal", "morton_keys", "permutation",

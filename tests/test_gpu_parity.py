@@ -15,8 +15,8 @@ from parity import (check_fields, dam_break_scene, field_close, hash_cell_map, o
 pytestmark = pytest.mark.gpu
 
 
-def check_step(p, bx, pos, vel, bpos, delta, with_fields=True, nbr_cap=None):
-    got = run_one_step(p, bx, pos, vel, bpos, delta)
+def check_step(p, bx, pos, vel, bpos, delta, with_fields=True, nbr_cap=None, config=None):
+    got = run_one_step(p, bx, pos, vel, bpos, delta, config=config)
     ref, bs, bm = oracle_one_step(p, bx, pos, vel, bpos, delta, nbr_cap=nbr_cap)
     n = pos.shape[0]
     # integer work: bit-exact
@@ -56,6 +56,26 @@ def check_step(p, bx, pos, vel, bpos, delta, with_fields=True, nbr_cap=None):
 def test_dam_break_with_walls():
     p, bx, pos, bpos = dam_break_scene(dims=(16, 16, 16))
     check_step(p, bx, pos, np.zeros_like(pos), bpos, 1e-3)
+
+
+@pytest.mark.parametrize("width", [0, 8, 32])
+def test_neighbour_list_widths(width):
+    # 0: the force and surface passes walk the density pass's bit matrix;
+    # 8 / 32: lists too short for all / some particles, whose rows are
+    # recomputed from their cell neighbourhoods (the default width fits all)
+    p, bx, pos, bpos = dam_break_scene(dims=(16, 16, 16))
+    vel = wcsph.make_velocities(pos.shape[0], 0.3, seed=9)
+    check_step(p, bx, pos, vel, bpos, 1e-3, config={"neighbour_list_width": width})
+
+
+def test_dense_cell_short_lists():
+    rng = np.random.default_rng(1)
+    pos = np.zeros((500, 4), np.float32)
+    pos[:, :3] = (0.3 + rng.random((500, 3)) * 0.06).astype(np.float32)
+    pos[:, 3] = 1.0
+    p = wcsph.default_params(particle_radius=0.01, max_time_step=1e-3, cfl_factor=0.0)
+    bx = wcsph.box((0, 0, 0), (1, 1, 1))
+    check_step(p, bx, pos, np.zeros_like(pos), None, 1e-3, config={"neighbour_list_width": 40, "mask_words": 4})
 
 
 def test_dam_break_no_walls_cfl_random_velocity():
