@@ -74,7 +74,7 @@ struct BatchSim {
     DevBuf<float> rho, prs, partials, metric_sums;
     DevBuf<u32> group_done;
     DevBuf<double> group_partials;
-    DevBuf<float4> xq, vq, xr;
+    DevBuf<float4> recf, recs;
     DevBuf<float4> ap, normal, vlap, anp;
     DevBuf<DevState> st;
     DevBuf<DevScene> scenes;
@@ -117,7 +117,7 @@ struct BatchSim {
         a.nbr_cnt = nbr_cnt.ptr;
         a.nbr_width = static_cast<u32>(nbr_width);
         a.rho = rho.ptr; a.prs = prs.ptr;
-        a.xq = xq.ptr; a.vq = vq.ptr; a.xr = xr.ptr;
+        a.recf = recf.ptr; a.recs = recs.ptr;
         a.ap = ap.ptr; a.normal = normal.ptr; a.vlap = vlap.ptr; a.anp = anp.ptr;
         a.pos_out = pos_a.ptr; a.vel_out = vel_a.ptr;
         a.box = nullptr;
@@ -259,7 +259,7 @@ static void build_batch(BatchSim& B, const wcsph_params& p, const wcsph_batch_sc
     if (n * static_cast<size_t>(B.nbr_width) >= (1ull << 32)) B.nbr_width = 0;   // 32-bit list slot indices
     B.nbr.alloc(n * static_cast<size_t>(B.nbr_width));
     B.nbr_cnt.alloc(n);
-    B.rho.alloc(n); B.prs.alloc(n); B.xq.alloc(n); B.vq.alloc(n); B.xr.alloc(n); B.ap.alloc(n); B.normal.alloc(n); B.vlap.alloc(n); B.anp.alloc(n);
+    B.rho.alloc(n); B.prs.alloc(n); B.recf.alloc(2 * n); B.recs.alloc(2 * n); B.ap.alloc(n); B.normal.alloc(n); B.vlap.alloc(n); B.anp.alloc(n);
     B.partials.alloc(2ull * pass_max_warps(B.n));
     B.group_done.alloc(pass_max_warps(B.n) / 32u + 1u);
     B.group_partials.alloc(2ull * (pass_max_warps(B.n) / 32u + 1u));

@@ -157,7 +157,7 @@ void CUDASPHSimulator::allocate() {
     offsets_.alloc(SORT_DIGITS * 256);
     lookback_.alloc(static_cast<size_t>(SORT_DIGITS) * sort_tiles(n_) * 256);
     perm_.alloc(n); ckey_.alloc(n); ckeys_.alloc(n);
-    rho_.alloc(n); prs_.alloc(n); xq_.alloc(n); vq_.alloc(n); xr_.alloc(n);
+    rho_.alloc(n); prs_.alloc(n); recf_.alloc(2 * n); recs_.alloc(2 * n);
     ap_.alloc(n); normal_.alloc(n); vlap_.alloc(n); anp_.alloc(n);
     st_.alloc(1); box_dev_.alloc(1); metrics_dev_.alloc(2);
     partials_.alloc(2ull * pass_max_warps(n_));
@@ -275,7 +275,7 @@ TravArgs CUDASPHSimulator::trav_args(float delta) {
     a.nbr_cnt = nbr_cnt_.ptr;
     a.nbr_width = static_cast<u32>(cfg_.nbr_width);
     a.rho = rho_.ptr; a.prs = prs_.ptr;
-    a.xq = xq_.ptr; a.vq = vq_.ptr; a.xr = xr_.ptr;
+    a.recf = recf_.ptr; a.recs = recs_.ptr;
     a.ap = ap_.ptr; a.normal = normal_.ptr; a.vlap = vlap_.ptr; a.anp = anp_.ptr;
     a.pos_out = pos_a_.ptr; a.vel_out = vel_a_.ptr;
     a.box = box_dev_.ptr;

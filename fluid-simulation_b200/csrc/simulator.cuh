@@ -192,7 +192,7 @@ private:
     DevBuf<u32> mask_;
     DevBuf<u32> nbr_, nbr_cnt_;  // neighbour lists (cfg_.nbr_width slots per particle) and counts
     DevBuf<float> rho_, prs_;
-    DevBuf<float4> xq_, vq_, xr_;
+    DevBuf<float4> recf_, recs_;   // neighbour records, two float4 per particle
     DevBuf<u64> ckeys_;         // order-equivalent short sort keys (radix_sort.cuh)
     DevBuf<float4> ap_, normal_, vlap_, anp_;
     DevBuf<float> partials_;

@@ -219,7 +219,7 @@ __device__ __forceinline__ void stage(const WarpView<KIND>& S, const TravArgs& a
 // A neighbour's data as the pair arithmetic reads it.
 //   x: position; FORCE: b = (v_j, 1 / rho_j), c = p_j / rho_j^2;
 //   SURFACE: b = n_j, c = rho_j; j: particle index (passes that address j).
-// Force and surface read two 16-byte records per neighbour (xq, vq / xr, normal).
+// Force and surface read one 32-byte record per neighbour (recf / recs).
 struct Nbr {
     float4 x, b;
     float c;
@@ -232,11 +232,11 @@ __device__ __forceinline__ Nbr fetch_j(const TravArgs& a, u32 j) {
     Nbr d;
     d.j = j;
     if constexpr (KIND == PASS_FORCE) {
-        d.x = __ldg(a.xq + j);
-        d.b = __ldg(a.vq + j);
+        d.x = __ldg(a.recf + 2 * static_cast<size_t>(j));
+        d.b = __ldg(a.recf + (2 * static_cast<size_t>(j) + 1));
     } else {
-        d.x = __ldg(a.xr + j);
-        d.b = __ldg(a.normal + j);
+        d.x = __ldg(a.recs + 2 * static_cast<size_t>(j));
+        d.b = __ldg(a.recs + (2 * static_cast<size_t>(j) + 1));
     }
     d.c = d.x.w;
     return d;
@@ -298,12 +298,13 @@ template <int KIND>
 __device__ __forceinline__ HomeData load_home(const TravArgs& a, u32 i) {
     HomeData H;
     if constexpr (KIND == PASS_FORCE) {
-        H.x = __ldg(a.xq + i);   // w = p / rho^2
-        H.v = __ldg(a.vq + i);
+        H.x = __ldg(a.recf + 2 * static_cast<size_t>(i));   // w = p / rho^2
+        H.v = __ldg(a.recf + (2 * static_cast<size_t>(i) + 1));
         H.prs = __ldg(a.prs + i);
         H.dpi = H.x.w;
     } else if constexpr (KIND == PASS_SURFACE) {
-        H.x = __ldg(a.xr + i);   // w = rho
+        H.x = __ldg(a.recs + 2 * static_cast<size_t>(i));   // w = rho
+        H.n = __ldg(a.recs + (2 * static_cast<size_t>(i) + 1));
         H.rho = H.x.w;
     } else {
         H.x = __ldg(a.pos + i);
@@ -314,7 +315,6 @@ __device__ __forceinline__ HomeData load_home(const TravArgs& a, u32 i) {
         H.prs = __ldg(a.prs + i);
         H.dpi = H.prs / (H.rho * H.rho);
     }
-    if constexpr (KIND == PASS_SURFACE) H.n = __ldg(a.normal + i);
     if constexpr (KIND == PASS_ADJ_FORCE) {
         H.abar = __ldg(a.adj_abar + i);
         H.w = __ldg(a.adj_w + i);
@@ -733,19 +733,21 @@ __device__ __forceinline__ void finish_row(const DevParams& P, const TravArgs& a
         // the force pass's neighbour records
         const float4 xi = a.pos[i];
         const float4 vi = a.vel[i];
-        a.xq[i] = make_float4(xi.x, xi.y, xi.z, prs / (rho * rho));
-        a.vq[i] = make_float4(vi.x, vi.y, vi.z, 1.f / rho);
+        a.recf[2 * static_cast<size_t>(i)] = make_float4(xi.x, xi.y, xi.z, prs / (rho * rho));
+        a.recf[2 * static_cast<size_t>(i) + 1] = make_float4(vi.x, vi.y, vi.z, 1.f / rho);
     } else if constexpr (KIND == PASS_FORCE) {
         // compute_pressure_accel_n_normal_with_boundary: m * sum_fluid, then
         // the boundary term (compute_pressure_accel_n_normal.cu:346-364)
         a.ap[i] = f4(P.mass * res[0] + resb[0], P.mass * res[1] + resb[1],
                      P.mass * res[2] + resb[2]);
         const float sn = P.h * P.mass;
-        a.normal[i] = f4(sn * res[3], sn * res[4], sn * res[5]);
+        const float4 ni = f4(sn * res[3], sn * res[4], sn * res[5]);
+        a.normal[i] = ni;
         a.vlap[i] = f4(res[6], res[7], res[8]);
         // the surface pass's neighbour record
         const float4 xi = a.pos[i];
-        a.xr[i] = make_float4(xi.x, xi.y, xi.z, a.rho[i]);
+        a.recs[2 * static_cast<size_t>(i)] = make_float4(xi.x, xi.y, xi.z, a.rho[i]);
+        a.recs[2 * static_cast<size_t>(i) + 1] = ni;
     } else if constexpr (KIND == PASS_SURFACE) {
         // a_np = g + F_ext + nu*10*m*vlap - alpha*2*rho0*f
         const float4 xi = a.pos[i];

@@ -80,10 +80,10 @@ struct TravArgs {
     // fields
     float* rho;
     float* prs;
-    // neighbour records packed for the gathers of the force and surface passes
-    float4* xq;               // (x, y, z, p / rho^2), written by the density pass
-    float4* vq;               // (vx, vy, vz, 1 / rho), written by the density pass
-    float4* xr;               // (x, y, z, rho), written by the force pass
+    // 32-byte neighbour records (one sector per neighbour) for the gathers of
+    // the force and surface passes, two float4 per particle
+    float4* recf;             // [2i] (x, y, z, p / rho^2), [2i+1] (v, 1 / rho); density pass
+    float4* recs;             // [2i] (x, y, z, rho), [2i+1] normal; force pass
     float4* ap;
     float4* normal;
     float4* vlap;
