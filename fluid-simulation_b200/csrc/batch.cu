@@ -83,7 +83,7 @@ struct BatchSim {
     DevBuf<u64> btable, bckey;
     DevBuf<u32> bcstart, bcend;
     u32 btable_size = 0;
-    int mask_words = 10;
+    int mask_words = 12;
     int nbr_width = 64;
 
     cudaGraphExec_t graph = nullptr;

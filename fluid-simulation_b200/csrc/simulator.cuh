@@ -74,7 +74,7 @@ struct StepConfig {
     int warps_density = 2;
     int warps_force = 4;
     int warps_surface = 2;
-    int mask_words = 10;        // neighbour bit-matrix words per particle (cap = 32*words)
+    int mask_words = 12;        // neighbour bit-matrix words per particle (cap = 32*words)
     int chunk = 0;              // sorted particles per warp: 8, 16, 32; 0 = by scene size
     int nbr_width = 64;         // neighbour-list slots per particle; 0 = walk the bit matrix
     float cell_size_mult = 1.f;
