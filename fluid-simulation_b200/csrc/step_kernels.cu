@@ -12,6 +12,7 @@ constexpr u32 FULL = 0xffffffffu;
 constexpr u32 BCAND_CAP = 256;   // boundary candidates expanded per warp and chunk
 constexpr u32 HOME_BLOCK = 32;   // home particles (bit-matrix rows) handled together
 constexpr u32 SEG_SLOTS = 64;    // segment partials, slot = lane + row (both < 32)
+constexpr u32 NO_HOME = 0xFFFFFFFFu;   // home rows not among the staged candidates
 
 
 __device__ __forceinline__ u32 lane_id() { return threadIdx.x & 31u; }
@@ -554,6 +555,19 @@ __device__ __forceinline__ u32 fluid_pair_run(const WarpView<KIND>& S, const Dev
     return c;
 }
 
+// Position of home row k of the density pass: from the staged candidates
+// (home_m0 = candidate index of row 0) when they hold the home cell, else
+// from global memory.
+__device__ __forceinline__ float4 home_x(const WarpView<PASS_DENSITY>& S, const TravArgs& a, u32 i0, u32 home_m0,
+                                         u32 k) {
+    if (home_m0 != NO_HOME) {
+        const u32 m = home_m0 + k;
+        const float* f = reinterpret_cast<const float*>(S.sp + pair_slot(m >> 1)) + (m & 1u);
+        return make_float4(f[0], f[2], f[4], 0.f);
+    }
+    return __ldg(a.pos + i0 + k);
+}
+
 // Neighbour pairs of rows [0, nh) read from the block's bit matrix in
 // global memory (bits, row length M), split by hits. Returns the run length
 // (0: no hits) and, for row k = lane, its hit range [lo, hi).
@@ -562,7 +576,17 @@ __device__ __forceinline__ u32 fluid_pair_run(const WarpView<KIND>& S, const Dev
 template <int KIND, bool SHARED_BITS = false>
 __device__ __forceinline__ u32 fluid_hit_run(const WarpView<KIND>& S, const DevParams& P, const TravArgs& a,
                                              const u32* __restrict__ bits, u32 nh, u32 M, u32 i0, u32& lo,
-                                             u32& hi, bool lists = false) {
+                                             u32& hi, bool lists = false, u32 home_m0 = NO_HOME) {
+    auto home = [&](u32 k) -> HomeData {
+        if constexpr (KIND == PASS_DENSITY) {
+            if (home_m0 != NO_HOME) {
+                HomeData H;
+                H.x = home_x(S, a, i0, home_m0, k);
+                return H;
+            }
+        }
+        return load_home<KIND>(a, i0 + k);
+    };
     auto ld = [&](u32 w) -> u32 {
         if constexpr (SHARED_BITS) return bits[w];
         else return __ldg(bits + w);
@@ -610,7 +634,7 @@ __device__ __forceinline__ u32 fluid_hit_run(const WarpView<KIND>& S, const DevP
             word = ld(++wr);
         }
         for (; r && word; --r) word &= word - 1;
-        HomeData H = load_home<KIND>(a, i0 + k);
+        HomeData H = home(k);
         float v[NF];
 #pragma unroll
         for (int f = 0; f < NF; ++f) v[f] = 0.f;
@@ -626,7 +650,7 @@ __device__ __forceinline__ u32 fluid_hit_run(const WarpView<KIND>& S, const DevP
 #pragma unroll
                 for (int f = 0; f < NF; ++f) v[f] = 0.f;
                 do { ++k; row0 += M; } while (p >= row0 + M);
-                H = load_home<KIND>(a, i0 + k);
+                H = home(k);
                 slot_base = hoff[k];
             }
             if constexpr (KIND == PASS_DENSITY) {
@@ -655,13 +679,13 @@ __device__ __forceinline__ u32 fluid_hit_run(const WarpView<KIND>& S, const DevP
 // (x_i - x_j is formed as fma(x_j, -1, x_i), the same single rounding).
 // The home particle's own bit is set here and cleared by the caller.
 __device__ __forceinline__ void density_test_words(const WarpView<PASS_DENSITY>& S, const DevParams& P,
-                                                   const TravArgs& a, u32 nh, u32 wpr, u32 i0) {
+                                                   const TravArgs& a, u32 nh, u32 wpr, u32 i0, u32 home_m0) {
     const u32 nwords = nh * wpr;
     const float2 neg = make_float2(-1.f, -1.f);
     for (u32 w = lane_id(); w < nwords; w += 32) {
         const u32 k = w / wpr;
         const u32 wi = w - k * wpr;
-        const float4 h = __ldg(a.pos + i0 + k);
+        const float4 h = home_x(S, a, i0, home_m0, k);
         const float2 X = make_float2(h.x, h.x), Y = make_float2(h.y, h.y), Z = make_float2(h.z, h.z);
         const float2* base = S.sp + pair_slot(wi * 16u);
         u32 bits = 0;
@@ -1201,7 +1225,8 @@ __global__ void __launch_bounds__(WPB * 32, KindCfg<KIND>::min_warps / WPB) cell
                         const u32 wpr = (len + 31u) >> 5;
                         const u32 len32 = wpr << 5;
                         const u32 nwords = nh * wpr;
-                        density_test_words(S, P, a, nh, wpr, i0);
+                        const u32 home_m0 = keep_bits ? self0 : NO_HOME;   // masked: the home cell is staged
+                        density_test_words(S, P, a, nh, wpr, i0, home_m0);
                         const u32 self = self0 + lane - c0;   // chunk index of the home particle itself
                         if (act && self < len) {
                             const u32 item = lane * len32 + self;
@@ -1210,7 +1235,7 @@ __global__ void __launch_bounds__(WPB * 32, KindCfg<KIND>::min_warps / WPB) cell
                         __syncwarp();
                         u32 lo, hi;
                         const u32 c = fluid_hit_run<KIND, true>(S, P, a, S.aux, nh, len32, i0, lo, hi,
-                                                                keep_bits && a.nbr != nullptr);
+                                                                keep_bits && a.nbr != nullptr, home_m0);
                         if (c) combine<NF>(S.part, res, act, lo, hi, c, lane);
                         if (keep_bits && hi - lo <= a.nbr_width) row_cnt = hi - lo;
                         if (keep_bits)
