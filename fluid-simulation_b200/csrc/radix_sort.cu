@@ -61,13 +61,23 @@ __global__ void keys_hist_kernel(const float4* __restrict__ pos, u32 n, float cs
 __global__ void keys_bounds_kernel(const float4* __restrict__ pos, u32 n, float cs, u64* __restrict__ keys_out,
                                    DevState* __restrict__ st) {
     int lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
-    for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const int3 c = cell_of(pos[i], cs);
+    auto take = [&](float4 x, u32 i) {
+        const int3 c = cell_of(x, cs);
         keys_out[i] = morton_key(c);
         lo[0] = min(lo[0], c.x); hi[0] = max(hi[0], c.x);
         lo[1] = min(lo[1], c.y); hi[1] = max(hi[1], c.y);
         lo[2] = min(lo[2], c.z); hi[2] = max(hi[2], c.z);
+    };
+    const u32 stride = gridDim.x * blockDim.x;
+    u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+    for (; i + 3 * stride < n; i += 4 * stride) {   // four loads in flight per thread
+        float4 x[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) x[u] = pos[i + u * stride];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) take(x[u], i + u * stride);
     }
+    for (; i < n; i += stride) take(pos[i], i);
     // warp, then block, then one atomic per axis and block
     __shared__ int s_lo[3], s_hi[3];
     if (threadIdx.x < 3) { s_lo[threadIdx.x] = 0; s_hi[threadIdx.x] = 0; }
@@ -105,18 +115,29 @@ __global__ void compressed_keys_hist_kernel(const float4* __restrict__ pos, u32 
     u32 valid_keys = 0;
     __syncthreads();
     const u32 stride = gridDim.x * blockDim.x;
-    for (u32 base = blockIdx.x * blockDim.x; base < n; base += stride) {   // uniform trip count (match.any)
-        const u32 i = base + threadIdx.x;
-        const bool valid = i < n;
-        u64 key = 0;
-        if (valid) {
-            const int3 c = cell_of(pos[i], cs);
-            key = part_by_3(static_cast<u32>(c.x + (1 << B))) | (part_by_3(static_cast<u32>(c.y + (1 << B))) << 1) |
-                  (part_by_3(static_cast<u32>(c.z + (1 << B))) << 2);
-            ckeys[i] = key;
-            ++valid_keys;
+    // uniform trip count per warp (match.any); four loads in flight per thread
+    for (u32 base = blockIdx.x * blockDim.x; base < n; base += 4 * stride) {
+        float4 x[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const u32 i = base + u * stride + threadIdx.x;
+            if (i < n) x[u] = pos[i];
         }
-        hist_add_key(s_hist, key, valid, ndigits);
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const u32 i = base + u * stride + threadIdx.x;
+            const bool valid = i < n;
+            u64 key = 0;
+            if (valid) {
+                const int3 c = cell_of(x[u], cs);
+                key = part_by_3(static_cast<u32>(c.x + (1 << B))) |
+                      (part_by_3(static_cast<u32>(c.y + (1 << B))) << 1) |
+                      (part_by_3(static_cast<u32>(c.z + (1 << B))) << 2);
+                ckeys[i] = key;
+                ++valid_keys;
+            }
+            hist_add_key(s_hist, key, valid, ndigits);
+        }
     }
     // the digits above ndigits: every key in bucket 0
     for (int o = 16; o > 0; o >>= 1) valid_keys += __shfl_xor_sync(0xffffffffu, valid_keys, o);
@@ -141,38 +162,45 @@ __global__ void hist_only_kernel(const u64* __restrict__ keys, u32 n, u32* __res
     flush_hist(s_hist, hist);
 }
 
-// One CTA of 256 threads: thread t owns digit value t of every pass.
+// One CTA of 256 threads (8 warps): digit offsets of every pass, and which
+// passes are trivial.
 __global__ void sort_plan_kernel(u32 n, u32* __restrict__ hist, u32* __restrict__ offsets,
                                  DevState* __restrict__ st) {
-    __shared__ u32 s_scan[256];
-    __shared__ u32 s_max[8];
+    // one warp per digit pass: lane l scans buckets 8l .. 8l + 7 serially,
+    // then the lanes' totals are scanned across the warp (no block barriers)
     __shared__ u32 s_active[SORT_DIGITS];
     const u32 t = threadIdx.x;
-    for (int p = 0; p < SORT_DIGITS; ++p) {
-        const u32 c = hist[p * 256 + t];
-        hist[p * 256 + t] = 0;  // ready for the next sort
-        // block exclusive scan (Hillis-Steele over 256 entries)
-        s_scan[t] = c;
-        __syncthreads();
-        for (u32 o = 1; o < 256; o <<= 1) {
-            const u32 v = t >= o ? s_scan[t - o] : 0u;
-            __syncthreads();
-            s_scan[t] += v;
-            __syncthreads();
+    const u32 pass = t >> 5;
+    const u32 lane = t & 31u;
+    if (pass < SORT_DIGITS) {
+        uint4* h = reinterpret_cast<uint4*>(hist + pass * 256 + lane * 8);
+        const uint4 h0 = h[0], h1 = h[1];
+        h[0] = make_uint4(0u, 0u, 0u, 0u);   // ready for the next sort
+        h[1] = make_uint4(0u, 0u, 0u, 0u);
+        const u32 c[8] = {h0.x, h0.y, h0.z, h0.w, h1.x, h1.y, h1.z, h1.w};
+        u32 ex[8];
+        u32 run = 0, mx = 0;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            ex[k] = run;
+            run += c[k];
+            mx = max(mx, c[k]);
         }
-        offsets[p * 256 + t] = s_scan[t] - c;
-        // max bucket: a pass is trivial when one bucket holds every key
-        u32 m = c;
-        for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
-        if ((t & 31) == 0) s_max[t >> 5] = m;
-        __syncthreads();
-        if (t == 0) {
-            u32 mx = 0;
-            for (int w = 0; w < 8; ++w) mx = max(mx, s_max[w]);
-            s_active[p] = (n > 0 && mx < n) ? 1u : 0u;
+        u32 incl = run;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const u32 v = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= static_cast<u32>(o)) incl += v;
         }
-        __syncthreads();
+        const u32 base = incl - run;
+        uint4* out = reinterpret_cast<uint4*>(offsets + pass * 256 + lane * 8);
+        out[0] = make_uint4(base + ex[0], base + ex[1], base + ex[2], base + ex[3]);
+        out[1] = make_uint4(base + ex[4], base + ex[5], base + ex[6], base + ex[7]);
+        // a pass is trivial when one bucket holds every key
+        mx = __reduce_max_sync(0xffffffffu, mx);
+        if (lane == 0) s_active[pass] = (n > 0 && mx < n) ? 1u : 0u;
     }
+    __syncthreads();
     if (t == 0) {
         u32 sel = 0;
         u32 first = SORT_DIGITS;
