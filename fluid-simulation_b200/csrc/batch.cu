@@ -256,7 +256,9 @@ static void build_batch(BatchSim& B, const wcsph_params& p, const wcsph_batch_sc
     B.table_size = static_cast<u32>(std::max<u64>(std::bit_ceil(static_cast<u64>(n)) / 4, 64) * p.table_size_mult);
     B.table.alloc(B.table_size); B.cstart.alloc(B.table_size); B.cend.alloc(B.table_size);
     B.mask.alloc(n * static_cast<size_t>(B.mask_words));
-    if (n * static_cast<size_t>(B.nbr_width) >= (1ull << 32)) B.nbr_width = 0;   // 32-bit list slot indices
+    // 32-bit list slot indices: fewer slots for very large ensembles, none below 8
+    if (n > 0) B.nbr_width = static_cast<int>(std::min<size_t>(static_cast<size_t>(B.nbr_width), ((1ull << 32) - 1) / n));
+    if (B.nbr_width < 8) B.nbr_width = 0;
     B.nbr.alloc(n * static_cast<size_t>(B.nbr_width));
     B.nbr_cnt.alloc(n);
     B.rho.alloc(n); B.prs.alloc(n); B.recf.alloc(2 * n); B.recs.alloc(2 * n); B.ap.alloc(n); B.normal.alloc(n); B.vlap.alloc(n); B.anp.alloc(n);

@@ -186,11 +186,14 @@ void CUDASPHSimulator::ensure_tables() {
     }
     const size_t words = static_cast<size_t>(n_) * static_cast<size_t>(cfg_.mask_words);
     if (mask_.count != words) mask_.alloc(words);
-    const size_t slots = static_cast<size_t>(n_) * static_cast<size_t>(cfg_.nbr_width);
-    if (slots >= (1ull << 32))   // list slots are addressed with 32-bit indices
-        throw Error(WCSPH_ERR_CONFIG, "neighbour_list_width * particles must stay below 2^32 (use a smaller width or 0)");
+    // list slots are addressed with 32-bit indices: very large scenes get
+    // fewer slots (rows that do not fit are recomputed), or none below 8
+    uint64_t width = static_cast<uint64_t>(cfg_.nbr_width);
+    if (n_ > 0) width = std::min<uint64_t>(width, ((1ull << 32) - 1) / n_);
+    nbr_width_ = width >= 8 ? static_cast<u32>(width) : 0u;
+    const size_t slots = static_cast<size_t>(n_) * nbr_width_;
     if (nbr_.count != slots) nbr_.alloc(slots);
-    const size_t counts = cfg_.nbr_width > 0 ? n_ : 0;
+    const size_t counts = nbr_width_ > 0 ? n_ : 0;
     if (nbr_cnt_.count != counts) nbr_cnt_.alloc(counts);
 }
 
@@ -271,9 +274,9 @@ TravArgs CUDASPHSimulator::trav_args(float delta) {
     a.mask = mask_.ptr;
     a.mask_words = static_cast<u32>(cfg_.mask_words);
     a.chunk = effective_chunk(cfg_, n_);
-    a.nbr = cfg_.nbr_width > 0 ? nbr_.ptr : nullptr;
+    a.nbr = nbr_width_ > 0 ? nbr_.ptr : nullptr;
     a.nbr_cnt = nbr_cnt_.ptr;
-    a.nbr_width = static_cast<u32>(cfg_.nbr_width);
+    a.nbr_width = nbr_width_;
     a.rho = rho_.ptr; a.prs = prs_.ptr;
     a.recf = recf_.ptr; a.recs = recs_.ptr;
     a.ap = ap_.ptr; a.normal = normal_.ptr; a.vlap = vlap_.ptr; a.anp = anp_.ptr;

@@ -190,7 +190,8 @@ private:
     DevBuf<u32> cstart_, cend_;
     uint32_t table_size_ = 0;
     DevBuf<u32> mask_;
-    DevBuf<u32> nbr_, nbr_cnt_;  // neighbour lists (cfg_.nbr_width slots per particle) and counts
+    DevBuf<u32> nbr_, nbr_cnt_;  // neighbour lists (nbr_width_ slots per particle) and counts
+    u32 nbr_width_ = 0;          // list slots in use: cfg_.nbr_width, capped so n * slots < 2^32
     DevBuf<float> rho_, prs_;
     DevBuf<float4> recf_, recs_;   // neighbour records, two float4 per particle
     DevBuf<u64> ckeys_;         // order-equivalent short sort keys (radix_sort.cuh)
