@@ -153,6 +153,21 @@ __device__ __forceinline__ u32 gather_ranges(u32* rstart, u32* rpref, u32 ncell,
     return total;
 }
 
+// Offset (dx, dy, dz) in [-R, R]^3 of neighbour cell q (x outermost, z
+// innermost: the reference's nesting order); R = 1 divides by a constant.
+__device__ __forceinline__ void cell_offset(u32 q, int R, int& dx, int& dy, int& dz) {
+    if (R == 1) {
+        dz = static_cast<int>(q % 3u) - 1;
+        dy = static_cast<int>((q / 3u) % 3u) - 1;
+        dx = static_cast<int>(q / 9u) - 1;
+    } else {
+        const u32 D = static_cast<u32>(2 * R + 1);
+        dz = static_cast<int>(q % D) - R;
+        dy = static_cast<int>((q / D) % D) - R;
+        dx = static_cast<int>(q / (D * D)) - R;
+    }
+}
+
 // Index of the range holding candidate m (rpref[lo] <= m < rpref[lo + 1]).
 __device__ __forceinline__ u32 range_of(const u32* rpref, u32 ncell, u32 m) {
     u32 lo = 0, hi = ncell;
@@ -504,7 +519,10 @@ template <int NF>
 __device__ __forceinline__ void combine(const float* part, float* res, bool active, u32 lo, u32 hi, u32 c,
                                         u32 k) {
     if (active && hi > lo) {
-        const u32 l_lo = lo / c, l_hi = (hi - 1) / c;
+        // x / c as a multiply-high, exact for x < 2^32 / c (x <= 32 c here)
+        const u32 inv = 0xFFFFFFFFu / c + 1u;
+        const u32 l_lo = c == 1u ? lo : __umulhi(lo, inv);
+        const u32 l_hi = c == 1u ? hi - 1 : __umulhi(hi - 1, inv);
         for (u32 l = l_lo; l <= l_hi; ++l) {
 #pragma unroll
             for (int f = 0; f < NF; ++f) res[f] += part[(l + k) * NF + f];
@@ -682,8 +700,10 @@ __device__ __forceinline__ void density_test_words(const WarpView<PASS_DENSITY>&
                                                    const TravArgs& a, u32 nh, u32 wpr, u32 i0, u32 home_m0) {
     const u32 nwords = nh * wpr;
     const float2 neg = make_float2(-1.f, -1.f);
+    // w / wpr as a multiply-high: exact for w < 2^32 / wpr^2 (here w < 32 * 16)
+    const u32 inv = 0xFFFFFFFFu / wpr + 1u;
     for (u32 w = lane_id(); w < nwords; w += 32) {
-        const u32 k = w / wpr;
+        const u32 k = wpr == 1u ? w : __umulhi(w, inv);
         const u32 wi = w - k * wpr;
         const float4 h = home_x(S, a, i0, home_m0, k);
         const float2 X = make_float2(h.x, h.x), Y = make_float2(h.y, h.y), Z = make_float2(h.z, h.z);
@@ -867,9 +887,8 @@ __device__ __forceinline__ void spill_row(const DevParams& P, const TravArgs& a,
 #pragma unroll
     for (int f = 0; f < NF; ++f) v[f] = 0.f;
     for (u32 q = lane; q < ncell; q += 32) {
-        const int dz = static_cast<int>(q % D) - R;
-        const int dy = static_cast<int>((q / D) % D) - R;
-        const int dx = static_cast<int>(q / (D * D)) - R;
+        int dx, dy, dz;
+        cell_offset(q, R, dx, dy, dz);
         u64 pk;
         if constexpr (BATCH) pk = pack_cell_batch(scene, ux + dx, uy + dy, uz + dz);
         else pk = pack_cell(ux + dx, uy + dy, uz + dz);
@@ -1105,9 +1124,8 @@ __global__ void __launch_bounds__(WPB * 32, KindCfg<KIND>::min_warps / WPB) cell
             }
             // fluid neighbour cells in the reference's x, y, z nesting order
             const u32 M = gather_ranges<BATCH>(S.rstart, S.rpref, ncell, a.fluid, [&](u32 q) {
-                const int dz = static_cast<int>(q % D) - R;
-                const int dy = static_cast<int>((q / D) % D) - R;
-                const int dx = static_cast<int>(q / (D * D)) - R;
+                int dx, dy, dz;
+                cell_offset(q, R, dx, dy, dz);
                 if constexpr (BATCH) return pack_cell_batch(scene, ux + dx, uy + dy, uz + dz);
                 else return pack_cell(ux + dx, uy + dy, uz + dz);
             });
