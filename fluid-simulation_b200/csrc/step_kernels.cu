@@ -242,18 +242,21 @@ struct Nbr {
     u32 j;
 };
 
+// A 32-byte record (two float4) in one 256-bit read-only load; the record
+// starts on a 32-byte boundary (the buffers are cudaMalloc'd, records are
+// 32 bytes).
+__device__ __forceinline__ void load_record(const float4* r, float4& x, float4& b) {
+    asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+        : "=f"(x.x), "=f"(x.y), "=f"(x.z), "=f"(x.w), "=f"(b.x), "=f"(b.y), "=f"(b.z), "=f"(b.w)
+        : "l"(r));
+}
+
 // Neighbour records of particle j (force and surface passes).
 template <int KIND>
 __device__ __forceinline__ Nbr fetch_j(const TravArgs& a, u32 j) {
     Nbr d;
     d.j = j;
-    if constexpr (KIND == PASS_FORCE) {
-        d.x = __ldg(a.recf + 2 * static_cast<size_t>(j));
-        d.b = __ldg(a.recf + (2 * static_cast<size_t>(j) + 1));
-    } else {
-        d.x = __ldg(a.recs + 2 * static_cast<size_t>(j));
-        d.b = __ldg(a.recs + (2 * static_cast<size_t>(j) + 1));
-    }
+    load_record((KIND == PASS_FORCE ? a.recf : a.recs) + 2 * static_cast<size_t>(j), d.x, d.b);
     d.c = d.x.w;
     return d;
 }
