@@ -317,13 +317,11 @@ template <int KIND>
 __device__ __forceinline__ HomeData load_home(const TravArgs& a, u32 i) {
     HomeData H;
     if constexpr (KIND == PASS_FORCE) {
-        H.x = __ldg(a.recf + 2 * static_cast<size_t>(i));   // w = p / rho^2
-        H.v = __ldg(a.recf + (2 * static_cast<size_t>(i) + 1));
+        load_record(a.recf + 2 * static_cast<size_t>(i), H.x, H.v);   // x.w = p / rho^2
         H.prs = __ldg(a.prs + i);
         H.dpi = H.x.w;
     } else if constexpr (KIND == PASS_SURFACE) {
-        H.x = __ldg(a.recs + 2 * static_cast<size_t>(i));   // w = rho
-        H.n = __ldg(a.recs + (2 * static_cast<size_t>(i) + 1));
+        load_record(a.recs + 2 * static_cast<size_t>(i), H.x, H.n);   // x.w = rho
         H.rho = H.x.w;
     } else {
         H.x = __ldg(a.pos + i);
