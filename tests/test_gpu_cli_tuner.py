@@ -151,3 +151,30 @@ def test_long_run_statistics_match_reference_kernels():
         m, t = float(np.mean(mine)), float(np.mean(theirs))
         print(f"{name}: time average {m:.6g} vs reference {t:.6g} ({(m - t) / t * 100:+.3f} %)")
         assert abs(m - t) <= 0.01 * abs(t)
+
+
+def test_traversal_config_names_round_trip(tmp_path):
+    """The traversal's own frozen-config names (bit-matrix words, particles
+    per warp, neighbour-list width) are read, applied and written back."""
+    p, bx, pos, bpos = dam_break_scene(dims=(10, 10, 10))
+    frozen = tmp_path / "traversal.json"
+    frozen.write_text(json.dumps([
+        {"Name": "mask_words", "Value": 8, "ValueType": "UnsignedInt"},
+        {"Name": "particles_per_warp", "Value": 16, "ValueType": "UnsignedInt"},
+        {"Name": "neighbour_list_width", "Value": 24, "ValueType": "UnsignedInt"},
+    ]))
+    sim = wcsph.CUDASPHSimulator(p, pos, bx, boundary_pos=bpos)
+    sim.set_tuning(wcsph.SEARCH_MCMC, 0.0, frozen)
+    sim.update(1e-3)
+    out = tmp_path / "saved.json"
+    sim.save_config(out)
+    sim.close()
+    saved = {e["Name"]: e["Value"] for e in json.loads(out.read_text())}
+    assert saved["mask_words"] == 8 and saved["particles_per_warp"] == 16 and saved["neighbour_list_width"] == 24
+    bad = tmp_path / "bad_width.json"
+    bad.write_text(json.dumps([{"Name": "neighbour_list_width", "Value": 5000, "ValueType": "UnsignedInt"}]))
+    sim = wcsph.CUDASPHSimulator(p, pos, bx, boundary_pos=bpos)
+    with pytest.raises(wcsph.WcsphError) as e:
+        sim.set_tuning(wcsph.SEARCH_MCMC, 0.0, bad)
+    assert e.value.status == wcsph.ERR_CONFIG and "neighbour_list_width" in e.value.message
+    sim.close()
