@@ -5,8 +5,8 @@
 //                   cells into the linear-probed hash (cell_start/cell_end)
 //                   (particle_data.cuh:130-131 + rebuild_n_search.cu:10-36)
 //   density pass    rho, Tait p (+boundary), the cell's neighbour bit matrix
-//                   over its candidate list and the packed neighbour records
-//                   of the force pass
+//                   over its candidate list, each particle's neighbour list
+//                   and the 32-byte neighbour records of the force pass
 //                   (compute_rho_p[_with_boundary], compute_rho_p.cu:192-318)
 //   force pass      pressure accel (+boundary), normals, viscosity Laplacian
 //                   (compute_pressure_accel_n_normal.cu:240-366 and the
@@ -15,9 +15,10 @@
 //                   CFL max |v|^2 and metric reductions
 //                   (compute_non_pressure_accel.cu + update_positions.cu:14-68)
 //
-// Work decomposition (all passes): one warp per chunk of 8, 16 or 32
-// particles of the sorted array (small scenes use small chunks so that more
-// warps run); for every cell that starts inside the chunk, the warp looks
+// Work decomposition (the density pass, and every pass when the lists are
+// off): one warp per chunk of 8, 16 or 32 particles of the sorted array
+// (small scenes use small chunks so that more warps run); for every cell
+// that starts inside the chunk, the warp looks
 // up the (2R+1)^3 neighbour cells once (lane-parallel hash probes) and
 // stages their particles (the candidates, in the reference's cell order)
 // into shared memory. The home particles are taken in blocks of up to 32.
@@ -34,9 +35,10 @@
 // (slot-major, so that a warp's rows read one slot coalesced), and the force
 // and surface passes no longer look at cells: lane k of a warp takes
 // particle k of the chunk and sums its list in order, then its boundary
-// cells. Rows whose neighbours did not fit (count > nbr_width, or a cell
-// beyond the bit-matrix capacity) carry NBR_SPILL and are recomputed from
-// their cell neighbourhood by the whole warp.
+// cells, gathering each neighbour's 32-byte record with one 256-bit load.
+// Rows whose neighbours did not fit (count > nbr_width, or a cell beyond
+// the bit-matrix capacity) carry NBR_SPILL and are recomputed from their
+// cell neighbourhood by the whole warp.
 // The bit-matrix walks split the block's neighbours into 32 contiguous lane
 // runs; each lane keeps one partial sum per home row it crosses and the
 // partials are added per home in lane order, so results are deterministic.
