@@ -139,6 +139,7 @@ CUDASPHSimulator::~CUDASPHSimulator() {
     for (cudaEvent_t e : box_done_)
         if (e) cudaEventDestroy(e);
     if (box_pinned_) cudaFreeHost(box_pinned_);
+    if (metrics_pinned_) cudaFreeHost(metrics_pinned_);
     tuner_.reset();
 }
 
@@ -488,9 +489,12 @@ void CUDASPHSimulator::reset() {
 }
 
 void CUDASPHSimulator::metrics(float* mean_speed, float* ke) {
-    float host[2] = {0.f, 0.f};
+    // read back through a small pinned buffer: a pageable destination would
+    // be staged by the driver on every call (this is read once per step)
+    if (!metrics_pinned_) WCSPH_CUDA(cudaMallocHost(&metrics_pinned_, sizeof(float) * 2));
+    float* host = metrics_pinned_;
     if (stepped_since_state_) {
-        WCSPH_CUDA(cudaMemcpyAsync(&host[0], &st_.ptr->last_mean_speed, sizeof(float) * 2, cudaMemcpyDeviceToHost,
+        WCSPH_CUDA(cudaMemcpyAsync(host, &st_.ptr->last_mean_speed, sizeof(float) * 2, cudaMemcpyDeviceToHost,
                                    stream_));
     } else {
         launch_metrics(vel_a_.ptr, n_, metric_mass_, metrics_dev_.ptr, stream_);

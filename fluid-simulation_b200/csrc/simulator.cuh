@@ -211,6 +211,7 @@ private:
     DevBox* box_pinned_ = nullptr;
     cudaEvent_t box_done_[kBoxSlots] = {};
     int box_slot_ = 0;
+    float* metrics_pinned_ = nullptr;   // 2 floats: the metrics read-back
     DevBuf<float> metrics_dev_;
     // boundary
     DevBuf<float4> bpos_;
