@@ -54,16 +54,26 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def measured_traffic(workload: str, n: int, kernel: str):
-    """DRAM bytes per launch of `kernel` from the committed ncu capture of this
-    workload (profiles/dram_traffic_<workload>.json), or None."""
+def _capture(workload: str, n: int):
     p = ROOT / "profiles" / f"dram_traffic_{workload}.json"
     if not p.exists():
         return None
     d = json.loads(p.read_text())
-    if d.get("particles") != n:
-        return None
-    return d["bytes_per_launch"].get(kernel)
+    return d if d.get("particles") == n else None
+
+
+def measured_traffic(workload: str, n: int, kernel: str):
+    """DRAM bytes per launch of `kernel` from the committed ncu capture of this
+    workload (profiles/dram_traffic_<workload>.json), or None."""
+    d = _capture(workload, n)
+    return None if d is None else d["bytes_per_launch"].get(kernel)
+
+
+def measured_limits(workload: str, n: int, kernel: str):
+    """Issue-active and L1TEX fractions of `kernel` from the same capture:
+    what bounds a kernel whose HBM fraction is low."""
+    d = _capture(workload, n)
+    return None if d is None else d.get("utilisation", {}).get(kernel)
 
 
 class ClockSampler:
@@ -269,6 +279,7 @@ def run_ours(args, world, rank, local, dist):
         "gpu_launches": launches,
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic,
+                     "ncu_utilisation": measured_limits(args.workload, n, dom),
                      "stage_ms": stage_ms},
     }
     line.update(extras)
