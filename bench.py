@@ -284,7 +284,8 @@ def run_ours(args, world, rank, local, dist):
     }
     line.update(extras)
     if not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(pre, args.cpu_budget)
+        # timed on rank 0 of a single-GPU run only (a bounded host sample)
+        line["cpu_baseline"] = cpu_baseline(pre, args.cpu_budget) if world == 1 else None
     return line
 
 
