@@ -112,7 +112,7 @@ struct BatchSim {
         a.boundary = HashView{btable.ptr, bcstart.ptr, bcend.ptr, btable_size ? btable_size - 1 : 0};
         a.mask = mask.ptr;
         a.mask_words = static_cast<u32>(mask_words);
-        a.chunk = n < (1u << 18) ? 8u : 32u;
+        a.chunk = n < (1u << 18) ? 8u : 16u;
         a.nbr = nbr_width > 0 ? nbr.ptr : nullptr;
         a.nbr_cnt = nbr_cnt.ptr;
         a.nbr_width = static_cast<u32>(nbr_width);

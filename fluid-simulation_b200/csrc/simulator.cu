@@ -73,7 +73,7 @@ DevParams make_dev_params(const wcsph_params& p) {
 
 uint32_t effective_chunk(const StepConfig& c, uint32_t n) {
     if (c.chunk == 8 || c.chunk == 16 || c.chunk == 32) return static_cast<uint32_t>(c.chunk);
-    return n < (1u << 18) ? 8u : 32u;
+    return n < (1u << 18) ? 8u : 16u;
 }
 
 float metric_mass(const wcsph_params& p) {

@@ -82,7 +82,8 @@ struct StepConfig {
     bool operator==(const StepConfig&) const = default;
 };
 // Particles per warp chunk of the traversal passes: the configured value, or
-// 8 below 2^18 particles (more warps for small scenes) and 32 above.
+// 8 below 2^18 particles (more warps for small scenes) and 16 above. The
+// list kernels take 32 particles per warp unless the chunk is 8.
 uint32_t effective_chunk(const StepConfig& c, uint32_t n);
 
 

@@ -1314,6 +1314,10 @@ __global__ void __launch_bounds__(WPB * 32, KindCfg<KIND>::min_warps / WPB) cell
     if constexpr (KIND == PASS_SURFACE) surface_reduce<WPB>(a, dt, np_dt, red_max, red_speed, red_speed2);
 }
 
+// Particles per warp of the list kernels: one per lane, except for small
+// scenes (density chunks of 8), which keep 8 so that more warps run.
+__host__ __device__ inline u32 list_rows_per_warp(u32 chunk) { return chunk == 8u ? 8u : 32u; }
+
 // Resident warps per SM the register allocation of the list kernels must
 // allow (32 -> 64 registers, 40 -> 48).
 template <int KIND>
@@ -1335,9 +1339,10 @@ __global__ void __launch_bounds__(WPB * 32, ListCfg<KIND>::min_warps / WPB) list
         np_dt = a.delta < a.np_max_dt ? a.delta : a.np_max_dt;
     }
     float red_max = 0.f, red_speed = 0.f, red_speed2 = 0.f;
-    const u32 base = (blockIdx.x * WPB + warp) * a.chunk;
+    const u32 rows = list_rows_per_warp(a.chunk);
+    const u32 base = (blockIdx.x * WPB + warp) * rows;
     if (base < a.n)
-        list_rows<KIND, BATCH>(P, a, base, min(a.chunk, a.n - base), dt, np_dt, red_max, red_speed, red_speed2);
+        list_rows<KIND, BATCH>(P, a, base, min(rows, a.n - base), dt, np_dt, red_max, red_speed, red_speed2);
     if constexpr (KIND == PASS_SURFACE) surface_reduce<WPB>(a, dt, np_dt, red_max, red_speed, red_speed2);
 }
 
@@ -1504,7 +1509,8 @@ static void launch_wpb(const DevParams& P, const TravArgs& a, cudaStream_t strea
 
 template <int KIND, bool BATCH>
 static void launch_kind(const DevParams& P, const TravArgs& a, cudaStream_t stream, int wpb) {
-    const u32 grid = pass_grid(a.n, wpb, a.chunk);
+    const bool listed = (KIND == PASS_FORCE || KIND == PASS_SURFACE) && a.nbr != nullptr;
+    const u32 grid = pass_grid(a.n, wpb, listed ? list_rows_per_warp(a.chunk) : a.chunk);
     if (grid == 0) return;
     switch (wpb) {
     case 2: launch_wpb<KIND, 2, BATCH>(P, a, stream, grid); break;

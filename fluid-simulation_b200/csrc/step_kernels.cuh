@@ -34,7 +34,8 @@
 // particle's neighbours, in candidate order, to its nbr_width list slots
 // (slot-major, so that a warp's rows read one slot coalesced), and the force
 // and surface passes no longer look at cells: lane k of a warp takes
-// particle k of the chunk and sums its list in order, then its boundary
+// particle k of the warp's 32 consecutive particles (8 when the density
+// chunk is 8) and sums its list in order, then its boundary
 // cells, gathering each neighbour's 32-byte record with one 256-bit load.
 // Rows whose neighbours did not fit (count > nbr_width, or a cell beyond
 // the bit-matrix capacity) carry NBR_SPILL and are recomputed from their

@@ -11,7 +11,7 @@ namespace wcsph {
 
 namespace {
 const int kWarps[] = {2, 4, 8};
-const int kMaskWords[] = {8, 10, 12, 16};
+const int kMaskWords[] = {8, 10, 11, 12, 16};
 const int kChunk[] = {8, 16, 32};
 const double kCellMult[] = {0.5, 2. / 3., 1., 1.5, 2.};  // step_tuner.cuh:88
 const uint32_t kTableMult[] = {1, 2, 4, 8, 16, 32};      // step_tuner.cuh:251-256
@@ -222,7 +222,7 @@ int Tuner::next_candidate() {
         case 0: shift(c.warps_density, kWarps, 3); break;
         case 1: shift(c.warps_force, kWarps, 3); break;
         case 2: shift(c.warps_surface, kWarps, 3); break;
-        case 3: shift(c.mask_words, kMaskWords, 4); break;
+        case 3: shift(c.mask_words, kMaskWords, 5); break;
         case 6: shift(c.chunk, kChunk, 3); break;
         case 4: {
             int idx = 0;
