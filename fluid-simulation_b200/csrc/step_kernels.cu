@@ -658,7 +658,7 @@ __device__ __forceinline__ u32 fluid_hit_run(const WarpView<KIND>& S, const DevP
 #pragma unroll
         for (int f = 0; f < NF; ++f) v[f] = 0.f;
         // density lists: list slot of hit h is h - (first hit of its row); u32
-        // indices (n * nbr_width < 2^32 is checked on the host)
+        // indices (the host caps nbr_width so that n * nbr_width < 2^32)
         u32 slot_base = hoff[k];
         while (word) {
             const u32 b = __ffs(word) - 1;
