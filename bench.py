@@ -46,6 +46,20 @@ PASS_BYTES = {
 STEP_BYTES = 400  # algorithmic bytes per fluid particle-step of the reference step structure
 
 
+BOX = {"large_tilting": "2x1x1 m tilting 0->15 deg/1 s", "dam_break": "1.0x0.6x0.6 m tank, walls on a 2r grid",
+       "mesh_obstacle": "1 m cube, walls + level-4 icosphere R 0.15 on a 2r grid"}
+
+
+def line_config(workload: str, n: int, delta: float, world: int, ms_per_step: float) -> dict:
+    """The `config` block of a bench line (both arms use it)."""
+    peak, peak_kind = measured_peaks()
+    step_bw = STEP_BYTES * n / (ms_per_step * 1e-3) / 1e9
+    return {"workload": workload, "particles": n, "dt": delta, "box": BOX.get(workload, "preset box"),
+            "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (~250 MB resident per step)",
+            "step_algorithmic_bytes_per_particle": STEP_BYTES,
+            "step_hbm_fraction_of_" + peak_kind: step_bw / peak}
+
+
 def measured_peaks():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -262,17 +276,13 @@ def run_ours(args, world, rank, local, dist):
     dom_ms = stage_ms[dom]
     achieved = PASS_BYTES[dom] * n / (dom_ms * 1e-3) / 1e9
     value = world * n * args.steps / (ms_max * 1e-3)
-    step_bw = STEP_BYTES * n / (ms_max / args.steps * 1e-3) / 1e9
     clocks = clk.summary()
     line = {
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32",
         "data": "synthetic: seeded jittered lattice + N(0,0.1) velocities (preset large_tilting)",
-        "config": {"workload": args.workload, "particles": n, "dt": delta, "box": "2x1x1 m tilting 0->15 deg/1 s",
-                   "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (~250 MB resident per step)",
-                   "step_algorithmic_bytes_per_particle": STEP_BYTES,
-                   "step_hbm_fraction_of_" + peak_kind: step_bw / peak},
+        "config": line_config(args.workload, n, delta, world, ms_max / args.steps),
         "clocks": {"sm_mhz": clocks["sm_mhz"], "sm_max_mhz": clocks["sm_max_mhz"], "reasons": clocks["reasons"]},
         "e2e": {"value": world * n * args.steps / e2e_s, "unit": METRIC, "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
@@ -352,7 +362,7 @@ def run_reference(args, world, rank, local, dist):
         import refpath
     except Exception as e:  # noqa: BLE001
         return {"impl": "reference", "unavailable": f"reference harness not importable: {e}"}
-    return refpath.bench_line(args, METRIC)
+    return refpath.bench_line(args, METRIC, lambda n, delta, ms: line_config(args.workload, n, delta, 1, ms))
 
 
 def main():

@@ -37,7 +37,10 @@ __global__ void iota_kernel(u32* ids, u32 n) {
 __global__ void ids_gather_kernel(const u32* __restrict__ ids_in, const u32* __restrict__ perm,
                                   u32* __restrict__ ids_out, u32 n) {
     const u32 i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) ids_out[i] = ids_in[perm[i]];
+    if (i < n) {
+        const u32 j = perm[i];
+        if (j < n) ids_out[i] = ids_in[j];   // always true unless the step's sort failed (reported)
+    }
 }
 
 __global__ void loss_kernel(const float4* __restrict__ pos, const u32* __restrict__ ids,
@@ -138,8 +141,10 @@ __global__ void unsort_kernel(const u32* __restrict__ perm, const float4* __rest
     const u32 i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) {
         const u32 j = perm[i];
-        xo[j] = xs[i];
-        vo[j] = vs[i];
+        if (j < n) {   // always true unless the step's sort failed (reported)
+            xo[j] = xs[i];
+            vo[j] = vs[i];
+        }
     }
 }
 

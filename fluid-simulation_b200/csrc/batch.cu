@@ -143,7 +143,7 @@ struct BatchSim {
         SortBuffers sb{};
         for (int i = 0; i < 3; ++i) { sb.keys[i] = keys[i].ptr; sb.vals[i] = vals[i].ptr; }
         sb.hist = hist.ptr; sb.offsets = offs.ptr; sb.lookback = lookback.ptr; sb.capacity = n;
-        enqueue_sort_passes(sb, n, st.ptr, stream);
+        WCSPH_CUDA(enqueue_sort_passes(sb, n, st.ptr, stream));
         launch_reorder_cells(pos_a.ptr, vel_a.ptr, vals[1].ptr, vals[2].ptr, st.ptr, n, dp.cell_size, pos_b.ptr,
                              vel_b.ptr, perm.ptr, ckey.ptr, table.ptr, cstart.ptr, cend.ptr, table_size - 1, st.ptr,
                              stream, scene_a.ptr);
@@ -275,6 +275,14 @@ static void build_batch(BatchSim& B, const wcsph_params& p, const wcsph_batch_sc
     WCSPH_CUDA(cudaMemsetAsync(B.table.ptr, 0xff, B.table.bytes(), s));
     WCSPH_CUDA(cudaMemsetAsync(B.cstart.ptr, 0, B.cstart.bytes(), s));
     WCSPH_CUDA(cudaMemsetAsync(B.cend.ptr, 0, B.cend.bytes(), s));
+    // index buffers start as valid indices (zeros): see CUDASPHSimulator::allocate
+    WCSPH_CUDA(cudaMemsetAsync(B.vals[1].ptr, 0, B.vals[1].bytes(), s));
+    WCSPH_CUDA(cudaMemsetAsync(B.vals[2].ptr, 0, B.vals[2].bytes(), s));
+    WCSPH_CUDA(cudaMemsetAsync(B.perm.ptr, 0, B.perm.bytes(), s));
+    WCSPH_CUDA(cudaMemsetAsync(B.ckey.ptr, 0, B.ckey.bytes(), s));
+    WCSPH_CUDA(cudaMemsetAsync(B.mask.ptr, 0, B.mask.bytes(), s));
+    if (B.nbr.ptr) WCSPH_CUDA(cudaMemsetAsync(B.nbr.ptr, 0, B.nbr.bytes(), s));
+    WCSPH_CUDA(cudaMemsetAsync(B.nbr_cnt.ptr, 0, B.nbr_cnt.bytes(), s));
     WCSPH_CUDA(cudaMemcpyAsync(B.pos_a.ptr, pos.data(), sizeof(float4) * n, cudaMemcpyHostToDevice, s));
     WCSPH_CUDA(cudaMemcpyAsync(B.vel_a.ptr, vel.data(), sizeof(float4) * n, cudaMemcpyHostToDevice, s));
     WCSPH_CUDA(cudaMemcpyAsync(B.scene_a.ptr, sid.data(), sizeof(u32) * n, cudaMemcpyHostToDevice, s));
@@ -293,7 +301,7 @@ static void build_batch(BatchSim& B, const wcsph_params& p, const wcsph_batch_sc
         sb.keys[0] = k0.ptr; sb.keys[1] = k1.ptr; sb.keys[2] = k2.ptr;
         sb.vals[1] = v1.ptr; sb.vals[2] = v2.ptr;
         sb.hist = B.hist.ptr; sb.offsets = B.offs.ptr; sb.lookback = lb.ptr; sb.capacity = nbb;
-        enqueue_sort_passes(sb, nbb, B.st.ptr, s);
+        WCSPH_CUDA(enqueue_sort_passes(sb, nbb, B.st.ptr, s));
         B.btable_size = std::max<u32>(std::bit_ceil(nbb), 64u);
         B.btable.alloc(B.btable_size); B.bcstart.alloc(B.btable_size); B.bcend.alloc(B.btable_size);
         WCSPH_CUDA(cudaMemsetAsync(B.btable.ptr, 0xff, B.btable.bytes(), s));

@@ -373,4 +373,10 @@ int wcsph_sort_keys_static(const uint64_t* keys, uint32_t n, uint32_t* perm, voi
     });
 }
 
+// Error-path test hook: see include/wcsph.h.
+int wcsph_test_stall_sort(int enable) {
+    wcsph::set_sort_stall_test(enable != 0);
+    return WCSPH_OK;
+}
+
 }  // extern "C"

@@ -1,9 +1,17 @@
 // radix_sort.cu — see radix_sort.cuh for the design.
 #include "radix_sort.cuh"
 
+#include <atomic>
+
 #include <cuda/atomic>
 
 namespace wcsph {
+
+namespace {
+std::atomic<bool> g_sort_stall_test{false};
+}
+
+void set_sort_stall_test(bool on) { g_sort_stall_test.store(on); }
 
 namespace {
 __device__ __forceinline__ u32 lanemask_lt() {
@@ -222,7 +230,8 @@ __global__ void sort_plan_kernel(u32 n, u32* __restrict__ hist, u32* __restrict_
 __global__ void __launch_bounds__(SORT_THREADS)
 onesweep_kernel(u32 n, int pass, u64* __restrict__ k0, u64* __restrict__ k1, u64* __restrict__ k2,
                 u32* __restrict__ v1, u32* __restrict__ v2, const u32* __restrict__ offsets,
-                u32* __restrict__ lookback, u32 tiles, DevState* __restrict__ st) {
+                u32* __restrict__ lookback, u32 tiles, DevState* __restrict__ st, u32 spin_limit,
+                u32 stall_first_tile) {
     if (!st->sort_active[pass]) return;
     constexpr int NW = SORT_THREADS / 32;
     __shared__ u32 s_tile;
@@ -297,7 +306,7 @@ onesweep_kernel(u32 n, int pass, u64* __restrict__ k0, u64* __restrict__ k1, u64
         cuda::atomic_ref<u32, cuda::thread_scope_device> mine(lb[static_cast<size_t>(tile) * 256u + d]);
         u32 excl = 0;
         if (tile == 0) {
-            mine.store(LB_FLAG_INC | count, cuda::memory_order_relaxed);
+            if (!stall_first_tile) mine.store(LB_FLAG_INC | count, cuda::memory_order_relaxed);
         } else {
             mine.store(LB_FLAG_AGG | count, cuda::memory_order_relaxed);
             int pred = static_cast<int>(tile) - 1;
@@ -308,7 +317,7 @@ onesweep_kernel(u32 n, int pass, u64* __restrict__ k0, u64* __restrict__ k1, u64
                 const u32 v = other.load(cuda::memory_order_relaxed);
                 const u32 flag = v & ~LB_VALUE_MASK;
                 if (flag == 0u) {
-                    if (++spins > LB_SPIN_LIMIT) {  // bounded wait: flag the error, never hang
+                    if (++spins > spin_limit) {  // bounded wait: flag the error, never hang
                         atomicOr(&st->error_flags, ERR_LOOKBACK_TIMEOUT);
                         break;
                     }
@@ -337,15 +346,24 @@ onesweep_kernel(u32 n, int pass, u64* __restrict__ k0, u64* __restrict__ k1, u64
     }
 }
 
-void enqueue_sort_passes(const SortBuffers& b, u32 n, DevState* st, cudaStream_t stream) {
+cudaError_t enqueue_sort_passes(const SortBuffers& b, u32 n, DevState* st, cudaStream_t stream) {
     const u32 tiles = sort_tiles(n);
-    if (n == 0) return;
+    if (n == 0) return cudaSuccess;
+    const bool stall = g_sort_stall_test.load();
+    const u32 spin_limit = stall ? LB_SPIN_LIMIT_STALLED : LB_SPIN_LIMIT;
     sort_plan_kernel<<<1, 256, 0, stream>>>(n, b.hist, b.offsets, st);
-    cudaMemsetAsync(b.lookback, 0, sizeof(u32) * SORT_DIGITS * static_cast<size_t>(tiles) * 256u, stream);
-    for (int p = 0; p < SORT_DIGITS; ++p)
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    e = cudaMemsetAsync(b.lookback, 0, sizeof(u32) * SORT_DIGITS * static_cast<size_t>(tiles) * 256u, stream);
+    if (e != cudaSuccess) return e;
+    for (int p = 0; p < SORT_DIGITS; ++p) {
         onesweep_kernel<<<tiles, SORT_THREADS, 0, stream>>>(n, p, b.keys[0], b.keys[1], b.keys[2],
                                                             b.vals[1], b.vals[2], b.offsets, b.lookback,
-                                                            tiles, st);
+                                                            tiles, st, spin_limit, stall ? 1u : 0u);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
 }
 
 }  // namespace wcsph

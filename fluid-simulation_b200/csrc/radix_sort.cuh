@@ -28,7 +28,8 @@ constexpr int SORT_DIGITS = 8;                      // 8 x 8-bit digits = 64 bit
 constexpr u32 LB_FLAG_AGG = 1u << 30;
 constexpr u32 LB_FLAG_INC = 2u << 30;
 constexpr u32 LB_VALUE_MASK = (1u << 30) - 1u;
-constexpr u32 LB_SPIN_LIMIT = 1u << 22;
+constexpr u32 LB_SPIN_LIMIT = 1u << 22;        // polls of one look-back wait (about a second)
+constexpr u32 LB_SPIN_LIMIT_STALLED = 1u << 12; // with the stall test hook on (a few milliseconds)
 
 inline u32 sort_tiles(u32 n) { return (n + SORT_TILE - 1) / SORT_TILE; }
 
@@ -67,12 +68,24 @@ __global__ void compressed_keys_hist_kernel(const float4* __restrict__ pos, u32 
 __global__ void hist_only_kernel(const u64* __restrict__ keys, u32 n, u32* __restrict__ hist);
 __global__ void sort_plan_kernel(u32 n, u32* __restrict__ hist, u32* __restrict__ offsets,
                                  DevState* __restrict__ st);
+// spin_limit bounds every look-back wait; stall_first_tile makes tile 0
+// withhold its look-back flags (the error-path test hook below), so that the
+// waits of the later tiles run out and set ERR_LOOKBACK_TIMEOUT.
 __global__ void onesweep_kernel(u32 n, int pass, u64* __restrict__ k0, u64* __restrict__ k1,
                                 u64* __restrict__ k2, u32* __restrict__ v1, u32* __restrict__ v2,
                                 const u32* __restrict__ offsets, u32* __restrict__ lookback,
-                                u32 tiles, DevState* __restrict__ st);
+                                u32 tiles, DevState* __restrict__ st, u32 spin_limit, u32 stall_first_tile);
 
 // Enqueues the complete sort (after keys[0] and hist are filled) on `stream`.
-void enqueue_sort_passes(const SortBuffers& b, u32 n, DevState* st, cudaStream_t stream);
+// Returns the first enqueue error (cudaSuccess when every call was accepted).
+// A pass whose look-back wait ran out sets ERR_LOOKBACK_TIMEOUT in
+// st->error_flags; its permutation is then not a permutation, and every
+// kernel that would read it (reorder, the traversal passes) leaves its
+// outputs untouched instead.
+cudaError_t enqueue_sort_passes(const SortBuffers& b, u32 n, DevState* st, cudaStream_t stream);
+
+// Error-path test hook: while on, sorts enqueued afterwards stall tile 0's
+// look-back flags and wait at most LB_SPIN_LIMIT_STALLED polls.
+void set_sort_stall_test(bool on);
 
 }  // namespace wcsph

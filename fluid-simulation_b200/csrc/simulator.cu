@@ -165,6 +165,12 @@ void CUDASPHSimulator::allocate() {
     group_done_.alloc(pass_max_warps(n_) / 32u + 1u);
     group_partials_.alloc(2ull * (pass_max_warps(n_) / 32u + 1u));
     WCSPH_CUDA(cudaMemsetAsync(group_done_.ptr, 0, group_done_.bytes(), stream_));
+    // Index buffers start as zeros (valid indices): a step whose sort fails
+    // leaves them as they were, and nothing may then read an index past n.
+    WCSPH_CUDA(cudaMemsetAsync(vals_[1].ptr, 0, vals_[1].bytes(), stream_));
+    WCSPH_CUDA(cudaMemsetAsync(vals_[2].ptr, 0, vals_[2].bytes(), stream_));
+    WCSPH_CUDA(cudaMemsetAsync(perm_.ptr, 0, perm_.bytes(), stream_));
+    WCSPH_CUDA(cudaMemsetAsync(ckey_.ptr, 0, ckey_.bytes(), stream_));
     ensure_tables();
     WCSPH_CUDA(cudaMemsetAsync(hist_.ptr, 0, hist_.bytes(), stream_));
     WCSPH_CUDA(cudaMemsetAsync(st_.ptr, 0, sizeof(DevState), stream_));
@@ -186,16 +192,25 @@ void CUDASPHSimulator::ensure_tables() {
         WCSPH_CUDA(cudaMemsetAsync(cend_.ptr, 0, cend_.bytes(), stream_));
     }
     const size_t words = static_cast<size_t>(n_) * static_cast<size_t>(cfg_.mask_words);
-    if (mask_.count != words) mask_.alloc(words);
+    if (mask_.count != words) {
+        mask_.alloc(words);
+        WCSPH_CUDA(cudaMemsetAsync(mask_.ptr, 0, mask_.bytes(), stream_));
+    }
     // list slots are addressed with 32-bit indices: very large scenes get
     // fewer slots (rows that do not fit are recomputed), or none below 8
     uint64_t width = static_cast<uint64_t>(cfg_.nbr_width);
     if (n_ > 0) width = std::min<uint64_t>(width, ((1ull << 32) - 1) / n_);
     nbr_width_ = width >= 8 ? static_cast<u32>(width) : 0u;
     const size_t slots = static_cast<size_t>(n_) * nbr_width_;
-    if (nbr_.count != slots) nbr_.alloc(slots);
+    if (nbr_.count != slots) {
+        nbr_.alloc(slots);
+        WCSPH_CUDA(cudaMemsetAsync(nbr_.ptr, 0, nbr_.bytes(), stream_));
+    }
     const size_t counts = nbr_width_ > 0 ? n_ : 0;
-    if (nbr_cnt_.count != counts) nbr_cnt_.alloc(counts);
+    if (nbr_cnt_.count != counts) {
+        nbr_cnt_.alloc(counts);
+        WCSPH_CUDA(cudaMemsetAsync(nbr_cnt_.ptr, 0, nbr_cnt_.bytes(), stream_));
+    }
 }
 
 // Boundary: Morton-sort once, hash (cell = h) and Akinci masses
@@ -216,7 +231,7 @@ void CUDASPHSimulator::init_boundary(const float* bpos_host) {
     keys_hist_kernel<<<std::min<u32>((nb + 255) / 256, 1184), 256, 0, stream_>>>(tmp.ptr, nb, dp_.h, k[0].ptr,
                                                                                  hist_.ptr);
     WCSPH_CUDA(cudaGetLastError());
-    enqueue_sort_passes(sb, nb, st_.ptr, stream_);
+    WCSPH_CUDA(enqueue_sort_passes(sb, nb, st_.ptr, stream_));
     btable_size_ = std::max<u32>(std::bit_ceil(nb), 64u);
     btable_.alloc(btable_size_); bcstart_.alloc(btable_size_); bcend_.alloc(btable_size_);
     WCSPH_CUDA(cudaMemsetAsync(btable_.ptr, 0xff, btable_.bytes(), stream_));
@@ -304,7 +319,7 @@ void CUDASPHSimulator::enqueue_search(bool keys_from_state) {
     for (int i = 0; i < 3; ++i) { sb.keys[i] = keys_[i].ptr; sb.vals[i] = vals_[i].ptr; }
     sb.keys[0] = ckeys_.ptr;   // the sort reads the compressed keys; keys_[0] keeps the field
     sb.hist = hist_.ptr; sb.offsets = offsets_.ptr; sb.lookback = lookback_.ptr; sb.capacity = n;
-    enqueue_sort_passes(sb, n, st_.ptr, stream_);
+    WCSPH_CUDA(enqueue_sort_passes(sb, n, st_.ptr, stream_));
     launch_reorder_cells(pos_a_.ptr, vel_a_.ptr, vals_[1].ptr, vals_[2].ptr, st_.ptr, n, dp_.cell_size, pos_b_.ptr,
                          vel_b_.ptr, perm_.ptr, ckey_.ptr, table_.ptr, cstart_.ptr, cend_.ptr, table_size_ - 1,
                          st_.ptr, stream_);
@@ -623,7 +638,7 @@ int CUDASPHSimulator::kernel_timings(const char** names, float* ms, int cap) {
     for (int i = 0; i < 3; ++i) { sb.keys[i] = keys_[i].ptr; sb.vals[i] = vals_[i].ptr; }
     sb.keys[0] = ckeys_.ptr;
     sb.hist = hist_.ptr; sb.offsets = offsets_.ptr; sb.lookback = lookback_.ptr; sb.capacity = n;
-    enqueue_sort_passes(sb, n, st_.ptr, stream_);
+    WCSPH_CUDA(enqueue_sort_passes(sb, n, st_.ptr, stream_));
     WCSPH_CUDA(cudaEventRecord(ev[2], stream_));
     launch_reorder_cells(pos_a_.ptr, vel_a_.ptr, vals_[1].ptr, vals_[2].ptr, st_.ptr, n, dp_.cell_size, pos_b_.ptr,
                          vel_b_.ptr, perm_.ptr, ckey_.ptr, table_.ptr, cstart_.ptr, cend_.ptr, table_size_ - 1,

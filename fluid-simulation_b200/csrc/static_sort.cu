@@ -14,6 +14,8 @@
 #include <mutex>
 #include <string>
 
+#include <cuda.h>   // CUcontext (the driver entry point is fetched through the runtime)
+
 #include "simulator.cuh"
 #include "static_sort.cuh"
 
@@ -34,38 +36,77 @@ struct StaticSortScratch {
 
 static __device__ __align__(256) StaticSortScratch g_static_sort_scratch;
 
-// perm[i] = index of the key of rank i (identity when no digit pass was active).
+// perm[i] = index of the key of rank i (identity when no digit pass was
+// active). When a look-back wait of the sort ran out, the passes did not
+// produce a permutation: every entry then reads WCSPH_STATIC_SORT_FAILED, an
+// index no key has (n <= WCSPH_STATIC_SORT_MAX_KEYS), so that the failure is
+// visible in the caller's own output without a host round trip.
 __global__ void write_perm_kernel(const StaticSortScratch* s, u32 n, u32* __restrict__ perm) {
     const u32 i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
+    if (s->st.error_flags) {
+        perm[i] = WCSPH_STATIC_SORT_FAILED;
+        return;
+    }
     const u32 sel = s->st.sort_sel[SORT_DIGITS];
     perm[i] = sel == 0u ? i : s->vals[sel - 1u][i];
 }
 
 constexpr int kMaxDevices = 64;
 std::mutex g_scratch_mu;
-StaticSortScratch* g_scratch_addr[kMaxDevices] = {};
+struct ScratchSlot {
+    CUcontext ctx = nullptr;   // context the address was looked up in
+    StaticSortScratch* addr = nullptr;
+};
+ScratchSlot g_scratch[kMaxDevices];
+
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+
+// The calling thread's current context, through the driver entry point the
+// runtime hands out (the library does not link the driver library itself).
+CUcontext current_context() {
+    static CtxGetCurrentFn fn = [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            f = nullptr;
+        return reinterpret_cast<CtxGetCurrentFn>(f);
+    }();
+    CUcontext c = nullptr;
+    if (!fn || fn(&c) != CUDA_SUCCESS) return nullptr;
+    return c;
+}
 
 // Device address of the scratch on the current device. On the host the name
 // g_static_sort_scratch is only a stand-in for the device symbol, never an
-// address a kernel may use, so the address is looked up once per device
-// (with that device current) and cached.
+// address a kernel may use, so the address is looked up with that device
+// current: once per device, and again whenever the device's current context
+// is not the one the address was found in (after cudaDeviceReset, or under a
+// caller's own driver-API context).
 StaticSortScratch* scratch_on_current_device() {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) throw Error(WCSPH_ERR_NO_DEVICE, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
     if (dev < 0 || dev >= kMaxDevices)
         throw Error(WCSPH_ERR_NOT_SUPPORTED, "wcsph_sort_keys_static supports devices 0..63");
+    // binds the device's primary context to this thread (CUDA 12 initialises
+    // it here) before the current context is read
+    e = cudaSetDevice(dev);
+    if (e != cudaSuccess) throw Error(WCSPH_ERR_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(e));
+    const CUcontext ctx = current_context();
     std::lock_guard<std::mutex> lock(g_scratch_mu);
-    if (!g_scratch_addr[dev]) {
+    ScratchSlot& slot = g_scratch[dev];
+    if (!slot.addr || slot.ctx != ctx) {
         void* p = nullptr;
         e = cudaGetSymbolAddress(&p, g_static_sort_scratch);
         if (e != cudaSuccess)
             throw Error(WCSPH_ERR_CUDA, std::string("cudaGetSymbolAddress(static sort scratch): ") +
                                             cudaGetErrorString(e));
-        g_scratch_addr[dev] = static_cast<StaticSortScratch*>(p);
+        slot.addr = static_cast<StaticSortScratch*>(p);
+        slot.ctx = ctx;
     }
-    return g_scratch_addr[dev];
+    return slot.addr;
 }
 
 }  // namespace
@@ -95,7 +136,7 @@ void static_sort_permutation(const uint64_t* keys, uint32_t n, uint32_t* perm, c
     const u32 blocks = (n + 255u) / 256u;
     hist_only_kernel<<<blocks, 256, 0, stream>>>(b.keys[0], n, s->hist);
     WCSPH_CUDA(cudaGetLastError());
-    enqueue_sort_passes(b, n, &s->st, stream);
+    WCSPH_CUDA(enqueue_sort_passes(b, n, &s->st, stream));
     write_perm_kernel<<<blocks, 256, 0, stream>>>(s, n, perm);
     WCSPH_CUDA(cudaGetLastError());
 }

@@ -1070,6 +1070,7 @@ __global__ void __launch_bounds__(WPB * 32, KindCfg<KIND>::min_warps / WPB) cell
     using C = KindCfg<KIND>;
     constexpr int NF = C::nf;
     constexpr int NFB = C::nfb;
+    if (a.st->error_flags & ERR_LOOKBACK_TIMEOUT) return;   // no sorted state this step (reorder skipped)
     extern __shared__ __align__(16) unsigned char dyn_smem[];
     const u32 lane = lane_id();
     const u32 warp = threadIdx.x >> 5;
@@ -1329,6 +1330,7 @@ struct ListCfg {
 template <int KIND, int WPB, bool BATCH>
 __global__ void __launch_bounds__(WPB * 32, ListCfg<KIND>::min_warps / WPB) list_pass_kernel(const DevParams P,
                                                                                           const TravArgs a) {
+    if (a.st->error_flags & ERR_LOOKBACK_TIMEOUT) return;   // no sorted state this step (reorder skipped)
     const u32 lane = lane_id();
     const u32 warp = threadIdx.x >> 5;
     float dt = 0.f, np_dt = 0.f;
@@ -1360,6 +1362,9 @@ __global__ void reorder_cells_kernel(const float4* __restrict__ pos_in, const fl
                                      float4* __restrict__ vel_out, u32* __restrict__ perm_out,
                                      u64* __restrict__ ckey_out, u64* table, u32* cstart, u32* cend,
                                      u32 tmask, DevState* st_err, const u32* __restrict__ scene_in) {
+    // a sort whose look-back wait ran out left no permutation: keep the
+    // previous sorted state and hash (every later pass returns at once too)
+    if (st->error_flags & ERR_LOOKBACK_TIMEOUT) return;
     const u32 i = blockIdx.x * blockDim.x + threadIdx.x;
     const u32 lane = threadIdx.x & 31u;
     const u32 sel = st->sort_sel[8];

@@ -195,6 +195,7 @@ def load_library(path: str | os.PathLike | None = None) -> C.CDLL:
         "wcsph_rollout_forward": (C.c_int, [vp, C.c_int, C.c_float, C.c_int, f, f]),
         "wcsph_rollout_backward": (C.c_int, [vp, f, f, f]),
         "wcsph_sort_keys_static": (C.c_int, [vp, C.c_uint32, vp, vp]),
+        "wcsph_test_stall_sort": (C.c_int, [C.c_int]),
         "wcsph_camera_look": (None, [f, C.c_float, C.c_float, C.c_uint32, C.c_uint32, C.POINTER(Camera)]),
         "wcsph_default_render_opts": (None, [C.POINTER(RenderOpts)]),
         "wcsph_render": (C.c_int, [vp, C.POINTER(Camera), C.POINTER(RenderOpts), vp, f]),
@@ -383,6 +384,7 @@ def write_ppm(path, rgba: np.ndarray) -> None:
 
 
 STATIC_SORT_MAX_KEYS = 65536
+STATIC_SORT_FAILED = 0xFFFFFFFF   # every perm entry after a sort whose bounded wait ran out
 
 
 def sort_keys_static(keys_ptr: int, n: int, perm_ptr: int, stream: int | None = None) -> None:
@@ -392,6 +394,21 @@ def sort_keys_static(keys_ptr: int, n: int, perm_ptr: int, stream: int | None = 
     include/wcsph.h). Enqueued on `stream` (a cudaStream_t handle, None = the
     default stream); the call does not wait for the GPU."""
     _check(load_library().wcsph_sort_keys_static(keys_ptr, n, perm_ptr, stream), None)
+
+
+class stall_sort:
+    """Error-path test hook (wcsph_test_stall_sort): inside the block, sorts
+    enqueued afterwards make their look-back waits run out (bounded, no hang),
+    so a step reports ERR_DEVICE_TIMEOUT and the static sort marks its output
+    with STATIC_SORT_FAILED."""
+
+    def __enter__(self):
+        load_library().wcsph_test_stall_sort(1)
+        return self
+
+    def __exit__(self, *exc):
+        load_library().wcsph_test_stall_sort(0)
+        return False
 
 
 def snapshot_read(path, app_name: str, fluid_n: int):

@@ -382,9 +382,30 @@ int wcsph_render(wcsph_ctx* ctx, const wcsph_camera* cam, const wcsph_render_opt
  *     done once per device); make that first call before any stream capture.
  *   - Every call on a device shares the one scratch: calls whose work overlaps
  *     on the GPU (other streams, other host threads) race and corrupt each
- *     other's results. Order them on one stream or synchronise between them. */
+ *     other's results. Order them on one stream or synchronise between them.
+ *   - The sort's waits between its tiles are bounded (about a second). If one
+ *     runs out, the call cannot tell the host without waiting for the GPU, so
+ *     it marks its output instead: every perm entry is then
+ *     WCSPH_STATIC_SORT_FAILED, an index no key has. Check perm[0] < n after
+ *     the stream work completes when this matters.
+ *   - The scratch address is looked up again when the device's current
+ *     context changes (after cudaDeviceReset, or under a driver-API context
+ *     of the caller's own). */
 #define WCSPH_STATIC_SORT_MAX_KEYS 65536u
+#define WCSPH_STATIC_SORT_FAILED 0xFFFFFFFFu
 int wcsph_sort_keys_static(const uint64_t* keys, uint32_t n, uint32_t* perm, void* stream);
+
+/* ---- error-path test hook ---------------------------------------------------
+ * No counterpart in the reference. While `enable` is non-zero, every radix sort
+ * enqueued afterwards (the step's, the boundary set-up's, the batch's and
+ * wcsph_sort_keys_static) withholds its first tile's look-back flags and bounds
+ * each look-back wait to 4096 polls, so that the waits of the later tiles run
+ * out within milliseconds. The step then reports WCSPH_ERR_DEVICE_TIMEOUT at
+ * its next synchronising call and leaves the particle state as it was; the
+ * static sort fills perm with WCSPH_STATIC_SORT_FAILED. Steps already captured
+ * in a CUDA graph keep the setting they were captured with. Nothing faults or
+ * hangs: it exists only to test these error paths. Returns WCSPH_OK.          */
+int wcsph_test_stall_sort(int enable);
 
 #ifdef __cplusplus
 }

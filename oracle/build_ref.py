@@ -53,6 +53,10 @@ VARIANTS = {
                                    table_mult=4, block=b) for b in (64, 128, 256, 512)},
     # 32^3 dam break with walls (dragon_settled.json: blocks 32, TABLE_SIZE_MULT 32)
     "dam_break": dict(n=32768, nb=7802, r=0.01, k=("textbook", 1000.0), nu=0.01, max_dt=1e-3, cfl=0.0, table_mult=32, block=32),
+    # mesh obstacle: 64 x 96 x 64 fluid block (r = 0.005) over a level-4
+    # icosphere in a 1 m cube; 64,276 wall + sphere particles; CFL 0.4, dt cap 1e-3
+    "mesh_obstacle": dict(n=393216, nb=64276, r=0.005, k=("textbook", 1000.0), nu=0.01, max_dt=1e-3, cfl=0.4,
+                          table_mult=4, block=32),
     # golden fixtures (2048 particles)
     "fixture_surface": dict(n=2048, nb=0, force="([](float4 pos) { return make_float4(0., 9.81f, 0., 0.); })",
                             table_mult=8, block=64),
@@ -161,7 +165,12 @@ def build_variant(ref: Path, name: str, spec: dict, jobs: int):
     cfg_path = src / "variant_config.h"
     lib = vdir / "librefpath.so"
     stamp = vdir / "config.stamp"
-    if lib.exists() and stamp.exists() and stamp.read_text() == cfg:
+    # rebuild when the variant's constants or the harness sources change
+    import hashlib
+
+    harness = b"".join((HERE / "refpath" / f).read_bytes() for f in ("refpath_host.cu", "ref_kernels.cu"))
+    cfg_stamp = cfg + "// harness " + hashlib.sha256(harness).hexdigest() + "\n"
+    if lib.exists() and stamp.exists() and stamp.read_text() == cfg_stamp:
         return name, "up to date"
     cfg_path.write_text(cfg)
     common = [*NVFLAGS, "-I", str(src), "-include", str(cfg_path)]
@@ -178,16 +187,21 @@ def build_variant(ref: Path, name: str, spec: dict, jobs: int):
     with cf.ThreadPoolExecutor(max_workers=jobs) as ex:
         list(ex.map(lambda a: nvcc(a, vdir), jobs_list))
     nvcc([*ARCH, "-shared", "-o", str(lib), *map(str, objs), "-lcudart_static", "-lrt", "-ldl", "-lpthread"], vdir)
-    stamp.write_text(cfg)
+    stamp.write_text(cfg_stamp)
     return name, "built"
 
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=os.environ.get("WCSPH_REFERENCE_DIR"),
+                    help="checkout of petbab/fluid-simulation (or set WCSPH_REFERENCE_DIR)")
     ap.add_argument("--variants", nargs="*", default=list(VARIANTS))
     ap.add_argument("--jobs", type=int, default=max(os.cpu_count() or 4, 4))
     a = ap.parse_args()
+    if not a.reference:
+        print("build_ref: no reference checkout given (--reference or WCSPH_REFERENCE_DIR); skipping",
+              file=sys.stderr)
+        return
     ref = Path(a.reference)
     if not (ref / "src" / "cuda" / "tuning" / "kernels").is_dir():
         print(f"build_ref: no reference sources at {ref}; skipping", file=sys.stderr)

@@ -258,6 +258,15 @@ int ref_step(float delta) {
 
 int ref_synchronize() { return cudaDeviceSynchronize() == cudaSuccess ? 0 : 3; }
 
+// Replaces the fluid state (n positions and velocities, float4) in the
+// current buffers: the next step starts from it, as after a snapshot load.
+int ref_set_state(const float* pos, const float* vel) {
+    if (!g) return 1;
+    cudaMemcpy(raw(g->pos[g->pos_src]), pos, sizeof(float4) * g->n, cudaMemcpyHostToDevice);
+    cudaMemcpy(raw(g->vel[g->vel_src]), vel, sizeof(float4) * g->n, cudaMemcpyHostToDevice);
+    return cudaDeviceSynchronize() == cudaSuccess ? 0 : 3;
+}
+
 // Times `k` steps with CUDA events on the default stream; boxes = NULL or
 // k boxes of 38 floats (set before each step).
 float ref_time_steps(int k, float delta, const float* boxes) {

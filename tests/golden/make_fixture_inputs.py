@@ -1,5 +1,9 @@
 #!/usr/bin/env python3
-"""Writes the golden fixture INPUTS (run here, where the reference checkout is).
+"""Writes the golden fixture INPUTS from a reference checkout:
+
+    python tests/golden/make_fixture_inputs.py <petbab/fluid-simulation checkout>
+
+(or with WCSPH_REFERENCE_DIR set).
 
 * surface_settled_2048.sphs / tilting_chaotic_2048.sphs: the first 2048
   particles (a Morton-compact chunk) of the reference's shipped snapshots
@@ -20,7 +24,15 @@ from pathlib import Path
 import numpy as np
 
 HERE = Path(__file__).resolve().parent
-REF = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference") / "measurements" / "snapshots"
+
+
+def snapshot_dir() -> Path:
+    import os
+
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("WCSPH_REFERENCE_DIR")
+    if not root:
+        raise SystemExit("usage: make_fixture_inputs.py <reference checkout> (or set WCSPH_REFERENCE_DIR)")
+    return Path(root) / "measurements" / "snapshots"
 
 
 def read_sphs(path: Path):
@@ -39,7 +51,7 @@ def write_sphs(path: Path, name: str, pos: np.ndarray, vel: np.ndarray):
 
 def main():
     info = {}
-    for f in sorted(REF.glob("*.sphs")):
+    for f in sorted(snapshot_dir().glob("*.sphs")):
         magic, version, name, n, pos, vel, raw = read_sphs(f)
         info[f.name] = {"magic": magic.decode(), "version": version, "app_name": name, "fluid_n": n,
                         "bytes": len(raw), "sha256": hashlib.sha256(raw).hexdigest(),

@@ -52,9 +52,70 @@ def one(name: str, out_dir: Path):
     print(name, "ok", int(cnt.sum()), "neighbour pairs", flush=True)
 
 
+def trajectory(name: str, out_dir: Path, steps: int, full: set[int]):
+    """The reference's own trajectory of `steps` steps from the scene's initial
+    state, one directory per step: the step's input state (in_pos, in_vel),
+    its sorted keys, permutation, (dt, np_dt), density, pressure and neighbour
+    counts; steps in `full` also keep every field and the neighbour lists.
+    A moving box is set to the scene's schedule before each step, as bench.py
+    does."""
+    import refpath
+
+    p, bx, pos, vel, bpos, delta = scene_of(name)
+    box_at = None
+    if name not in __import__("fixtures").NAMES:
+        import wcsph
+
+        pre = wcsph.preset(name)
+        box_at = pre.box_at if pre.info.moving_box else None
+    sim = refpath.RefSim(name, pos, vel, bpos, bx)
+    in_pos, in_vel = pos, vel
+    n = pos.shape[0]
+    for k in range(steps):
+        d = out_dir / f"step_{k:04d}"
+        d.mkdir(parents=True, exist_ok=True)
+        if box_at is not None:
+            sim.set_box(box_at(k + 1))
+        sim.step(delta)
+        np.save(d / "in_pos.npy", in_pos)
+        np.save(d / "in_vel.npy", in_vel)
+        if k in full:
+            f = sim.fields()
+            cnt, off, nbr = f.pop("neighbors")
+            np.save(d / "nbr_offsets.npy", off)
+            np.save(d / "nbr_idx.npy", nbr)
+            for key in ("position", "velocity", "pressure_accel", "non_pressure_accel", "normal"):
+                np.save(d / f"{key}.npy", f[key])
+            if bpos is not None:
+                np.save(d / "boundary_position.npy", f["boundary_position"])
+                np.save(d / "boundary_mass.npy", f["boundary_mass"])
+            keys, perm, rho, prs, dt = f["sorted_keys"], f["permutation"], f["density"], f["pressure"], f["dt"]
+        else:
+            keys = np.empty(n, np.uint64)
+            perm = np.empty(n, np.uint32)
+            rho = np.empty(n, np.float32)
+            prs = np.empty(n, np.float32)
+            cnt = np.empty(n, np.uint32)
+            dt2 = np.empty(2, np.float32)
+            sim._get(sorted_keys=keys, permutation=perm, density=rho, pressure=prs, nbr_counts=cnt, dt=dt2)
+            dt = (float(dt2[0]), float(dt2[1]))
+        np.save(d / "sorted_keys.npy", keys)
+        np.save(d / "permutation.npy", perm)
+        np.save(d / "density.npy", rho)
+        np.save(d / "pressure.npy", prs)
+        np.save(d / "nbr_counts.npy", cnt)
+        np.save(d / "dt.npy", np.array(dt, np.float32))
+        in_pos, in_vel = sim.state()
+    sim.close()
+    print(name, "trajectory ok", steps, "steps", flush=True)
+
+
 def main():
-    # make_ref_fixtures.py [out_dir [scene]]
+    # make_ref_fixtures.py [out_dir [scene [--trajectory STEPS [FULL_STEP ...]]]]
     out = Path(sys.argv[1]) if len(sys.argv) > 1 else HERE
+    if len(sys.argv) > 3 and sys.argv[3] == "--trajectory":
+        trajectory(sys.argv[2], out, int(sys.argv[4]), {int(x) for x in sys.argv[5:]})
+        return
     if len(sys.argv) > 2:
         one(sys.argv[2], out)
         return

@@ -77,23 +77,58 @@ def pressure_bounds(p, rho, prs, spos, nbr, bpos=None, bmass=None, dt=0.0, tol=R
     return {"pressure": dp, "pressure_accel": da, "velocity": dt * da, "position": dt * dt * da}
 
 
-def check_fields(got: dict, want: dict, bounds: dict | None = None, tol=REL_TOL):
-    """-> list of failure strings (empty when every field is within tolerance)."""
-    fails = []
-    for f in ("density", "pressure", "pressure_accel", "non_pressure_accel", "normal", "position", "velocity"):
+FIELDS = ("density", "pressure", "pressure_accel", "non_pressure_accel", "normal", "position", "velocity")
+
+
+def field_report(got: dict, want: dict, bounds: dict | None = None, tol=REL_TOL, fields=FIELDS) -> dict:
+    """Per field: `plain` = worst |error| / (tol x field scale), the plain
+    field-scaled 1e-5 test; `widened` = the same against the plain bound plus
+    the propagated EOS bound (fields listed in `bounds` only)."""
+    out = {}
+    for f in fields:
         g = np.asarray(got[f], np.float64)
         w = np.asarray(want[f], np.float64)
         if g.ndim == 2:
             g, w = g[:, :3], w[:, :3]
         scale = np.max(np.abs(w)) if w.size else 0.0
         bound = tol * np.maximum(np.abs(w), scale) + 1e-30
+        err = np.abs(g - w)
+        r = {"plain": float(np.max(err / bound)) if g.size else 0.0}
         if bounds is not None and f in bounds:
             extra = np.asarray(bounds[f], np.float64)
-            bound = bound + (extra[:, None] if g.ndim == 2 else extra)
-        worst = float(np.max(np.abs(g - w) / bound)) if g.size else 0.0
-        if worst > 1.0:
-            fails.append(f"{f}: worst error {worst:.3g} x tolerance")
+            wide = bound + (extra[:, None] if g.ndim == 2 else extra)
+            r["widened"] = float(np.max(err / wide)) if g.size else 0.0
+        out[f] = r
+    _append_report(out)
+    return out
+
+
+def check_fields(got: dict, want: dict, bounds: dict | None = None, tol=REL_TOL, fields=FIELDS):
+    """-> list of failure strings (empty when every field is within tolerance).
+    A field passes under the plain field-scaled bound; only a field that
+    fails it and has a propagated EOS bound (pressure and what it drives) is
+    then held to the widened bound."""
+    fails = []
+    for f, r in field_report(got, want, bounds, tol, fields).items():
+        if r["plain"] <= 1.0:
+            continue
+        if "widened" in r and r["widened"] <= 1.0:
+            continue
+        fails.append(f"{f}: worst error {r['plain']:.3g} x the plain tolerance"
+                     + (f", {r['widened']:.3g} x the widened one" if "widened" in r else ""))
     return fails
+
+
+def _append_report(rep: dict):
+    """With WCSPH_PARITY_REPORT set, every comparison is appended to that
+    file as one JSON line (test id, per-field ratios) for the record."""
+    import json
+    import os
+
+    path = os.environ.get("WCSPH_PARITY_REPORT")
+    if path:
+        with open(path, "a") as fh:
+            fh.write(json.dumps({"test": os.environ.get("PYTEST_CURRENT_TEST", "?"), "fields": rep}) + "\n")
 
 
 def dam_break_scene(dims=(16, 16, 16), r=0.01, jitter_frac=0.1, seed=7, walls=True, tank=(1.0, 0.6, 0.6),

@@ -4,9 +4,15 @@ FP64 reverse-mode reference and FP64 central finite differences, on a
 r = 0.01, walls, 200 fixed 1e-3 steps, checkpoints every 20 steps,
 target = initial lattice + (0.2, 0, 0.1)).
 
-Tolerances: the FP32 forward drifts from the FP64 one over 200 steps, so the
-comparison is relative: |g_cuda - g_ref| <= GRAD_TOL * |g_ref| for dL/dnu
-and dL/dk, and ||g_cuda - g_ref|| <= VEC_TOL * ||g_ref|| for dL/dv0.
+Tolerances (the 1e-3 relative of the differentiable-rollout target):
+|g_cuda - g_ref| <= GRAD_TOL * |g_ref| for dL/dnu and dL/dk, and
+||g_cuda - g_ref|| <= VEC_TOL * ||g_ref|| for dL/dv0, against FP64 reverse
+mode and against FP64 central differences. The differences use a step that
+crosses no neighbour-set change (FD_STEP, relative for nu and k, absolute in
+m/s for v0): a pair entering or leaving the support radius inside the
+difference makes the loss jump, which a derivative does not see. The 1e-4
+step of the workload's specification crosses such a change for nu; its value
+is printed beside the converged one.
 """
 import numpy as np
 import pytest
@@ -16,8 +22,9 @@ import wcsph
 from adjoint_ref import Scene, fd_gradient, reference_gradients
 
 pytestmark = pytest.mark.gpu
-GRAD_TOL = 1e-2
-VEC_TOL = 5e-2
+GRAD_TOL = 1e-3
+VEC_TOL = 1e-3
+FD_STEP = 1e-6
 
 
 def rollout_scene(dims=(16, 16, 8)):
@@ -67,14 +74,21 @@ def test_adjoint_matches_finite_differences():
     loss, gv, gnu, gk, bpos, bmass = cuda_gradients(p, bx, pos, walls, target, steps, dt, 20)
     sc = Scene(p, bx, pos, np.zeros_like(pos), bpos, bmass.astype(np.float64))
     nu, k = float(p.viscosity), float(p.stiffness)
-    fnu = fd_gradient(sc, nu, k, steps, dt, target, "nu")
-    fk = fd_gradient(sc, nu, k, steps, dt, target, "k")
-    print(f"dL/dnu {gnu:.6g} fd {fnu:.6g}; dL/dk {gk:.6g} fd {fk:.6g}")
+    fnu = fd_gradient(sc, nu, k, steps, dt, target, "nu", step=FD_STEP)
+    fk = fd_gradient(sc, nu, k, steps, dt, target, "k", step=FD_STEP)
+    fnu_spec = fd_gradient(sc, nu, k, steps, dt, target, "nu", step=1e-4)
+    print(f"dL/dnu {gnu:.7g} fd({FD_STEP:g}) {fnu:.7g} (fd(1e-4) {fnu_spec:.7g}, crosses a neighbour-set change); "
+          f"dL/dk {gk:.7g} fd {fk:.7g}")
     assert abs(gnu - fnu) <= GRAD_TOL * abs(fnu)
     assert abs(gk - fk) <= GRAD_TOL * abs(fk)
+    # three components of dL/dv0 (particles at the corner, inside and at the far end of the block)
+    got, want = [], []
     for idx in ((5, 0), (1000, 1), (2000, 2)):
-        f = fd_gradient(sc, nu, k, steps, dt, target, "v0", index=idx)
-        assert abs(gv[idx] - f) <= GRAD_TOL * max(abs(f), 1e-9) + 1e-7, (idx, gv[idx], f)
+        want.append(fd_gradient(sc, nu, k, steps, dt, target, "v0", index=idx, step=FD_STEP))
+        got.append(float(gv[idx]))
+    got, want = np.array(got), np.array(want)
+    print("dL/dv0 components", got, "fd", want)
+    assert np.linalg.norm(got - want) <= VEC_TOL * np.linalg.norm(want)
 
 
 def test_rollout_restores_final_state_and_is_repeatable():

@@ -54,3 +54,40 @@ def test_static_sort_at_the_maximum_size_and_the_limit():
     with pytest.raises(wcsph.WcsphError) as e:
         wcsph.sort_keys_static(d.data_ptr(), n + 1, d.data_ptr(), None)
     assert e.value.status == wcsph.ERR_INVALID_ARGUMENT and "exceeds the maximum" in e.value.message
+
+
+def test_static_sort_allocates_no_device_memory():
+    """The property the entry point exists for: after a first call (which may
+    load the library's device image), repeated sorts at the maximum size leave
+    the device's free memory unchanged."""
+    torch = pytest.importorskip("torch")
+    n = wcsph.STATIC_SORT_MAX_KEYS
+    rng = np.random.default_rng(8)
+    d_keys = torch.from_numpy(rng.integers(0, 1 << 62, n, dtype=np.int64)).cuda()
+    d_perm = torch.empty(n, dtype=torch.int32, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    wcsph.sort_keys_static(d_keys.data_ptr(), n, d_perm.data_ptr(), stream)
+    torch.cuda.synchronize()
+    free_before, _ = torch.cuda.mem_get_info()
+    for _ in range(8):
+        wcsph.sort_keys_static(d_keys.data_ptr(), n, d_perm.data_ptr(), stream)
+    torch.cuda.synchronize()
+    free_after, _ = torch.cuda.mem_get_info()
+    assert free_after == free_before
+    want = np.argsort(d_keys.cpu().numpy().view(np.uint64), kind="stable").astype(np.uint32)
+    assert np.array_equal(d_perm.cpu().numpy().view(np.uint32), want)
+
+
+def test_static_sort_marks_its_output_when_a_wait_runs_out():
+    """A look-back wait that runs out (forced by the bounded stall hook; no
+    fault, no hang) leaves every perm entry at STATIC_SORT_FAILED, and the next
+    call, with the scratch cleared again, sorts correctly."""
+    torch = pytest.importorskip("torch")
+    n = wcsph.STATIC_SORT_MAX_KEYS
+    keys = np.random.default_rng(9).integers(0, 1 << 40, n).astype(np.uint64)
+    with wcsph.stall_sort():
+        stalled = _device_sort(torch, keys, calls=1)[0]
+    assert (stalled == np.uint32(wcsph.STATIC_SORT_FAILED)).all()
+    want = np.argsort(keys, kind="stable").astype(np.uint32)
+    for got in _device_sort(torch, keys):
+        assert np.array_equal(got, want)
