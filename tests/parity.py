@@ -67,13 +67,15 @@ def pressure_bounds(p, rho, prs, spos, nbr, bpos=None, bmass=None, dt=0.0, tol=R
     gw = grad_norm(x[i] - x[idx])
     da = mass * np.bincount(i, weights=(dp[i] / rho[i] ** 2 + dp[idx] / rho[idx] ** 2) * gw, minlength=len(rho))
     if bpos is not None and len(bpos):
+        from scipy.spatial import cKDTree
+
         b = np.asarray(bpos, np.float64)[:, :3]
-        for s0 in range(0, len(x), 4096):
-            xs = x[s0:s0 + 4096]
-            d = xs[:, None, :] - b[None, :, :]
-            g = grad_norm(d)
-            w = np.asarray(bmass, np.float64)[None, :] * g
-            da[s0:s0 + 4096] += (dp[s0:s0 + 4096] * (1 / rho[s0:s0 + 4096] ** 2 + 1 / rho0 ** 2)) * w.sum(1)
+        # fluid-boundary pairs within h (a superset of the kernel's support is harmless: the gradient is 0 beyond h)
+        pairs = cKDTree(x).sparse_distance_matrix(cKDTree(b), h * (1 + 1e-6), output_type="coo_matrix")
+        q = pairs.data / h
+        g = np.where((q >= 1e-9) & (q <= 1.0), np.abs(spiky) * (1 - q) ** 2 / h, 0.0)   # |grad W| = |g| |r|
+        w = np.bincount(pairs.row, weights=np.asarray(bmass, np.float64)[pairs.col] * g, minlength=len(x))
+        da += dp * (1 / rho ** 2 + 1 / rho0 ** 2) * w
     return {"pressure": dp, "pressure_accel": da, "velocity": dt * da, "position": dt * dt * da}
 
 
