@@ -44,7 +44,7 @@ struct SortBuffers {
 
 // Computes Morton keys of `pos` (cell = floorf(p / cs), particle_data.cuh:117-125)
 // into keys[0] and accumulates the 8 digit histograms.
-// With `scene` (batched ensembles) the key is batch_key(scene[i], morton).
+// With `scene` (batched ensembles) the key is batch_key(scene[i], cell).
 __global__ void keys_hist_kernel(const float4* __restrict__ pos, u32 n, float cs,
                                  u64* __restrict__ keys_out, u32* __restrict__ hist,
                                  const u32* __restrict__ scene = nullptr);

@@ -81,14 +81,17 @@ __host__ __device__ __forceinline__ float4 mat_mul(const float4 m[4], float4 v) 
 }
 
 // Squared distance used by the neighbour predicate (is_neighbor,
-// common.cuh:39-47). The rounding is fixed explicitly (x*x first, then y and
-// z fused) so that the CUDA path, the oracle and every pass see the same
-// neighbour set; the oracle evaluates the identical fma chain.
+// common.cuh:39-47, with dot() of math.cuh:54-56). The reference's
+// a.x*b.x + a.y*b.y + a.z*b.z is contracted by nvcc to
+// fma(z, z, fma(x, x, y*y)): y*y is rounded first, then x and z are fused in.
+// The rounding is fixed here explicitly in that order so that the CUDA path,
+// the oracle (the identical fma chain) and the reference's kernels decide
+// pairs at |r| = h alike; other orders differ from it by one ulp on such pairs.
 __device__ __forceinline__ float dist2(float4 a, float4 b) {
     const float dx = __fsub_rn(a.x, b.x);
     const float dy = __fsub_rn(a.y, b.y);
     const float dz = __fsub_rn(a.z, b.z);
-    return __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmul_rn(dx, dx)));
+    return __fmaf_rn(dz, dz, __fmaf_rn(dx, dx, __fmul_rn(dy, dy)));
 }
 
 // ------------------------------------------------------------ SPH kernels --
@@ -204,9 +207,9 @@ __host__ __device__ __forceinline__ u64 cell_hash_packed(u64 pk) {
                      static_cast<u32>((pk >> 42) & 0x1FFFFFull));
 }
 
-// Batched ensembles key cells by (scene, cell): 16 bits per axis of the offset
-// coordinates plus the scene id in bits 48..62. Scenes must lie inside one
-// 65536-cell window per axis (checked at creation).
+// Batched ensembles key cells by (scene, cell): the low 16 bits per axis of
+// the offset coordinates plus the scene id in bits 48..62, unique for cell
+// coordinates in [-2^15, 2^15) (checked at creation).
 __host__ __device__ __forceinline__ u64 pack_cell_batch(u32 scene, u32 x, u32 y, u32 z) {
     return (static_cast<u64>(scene) << 48) | static_cast<u64>(x & 0xFFFFu) |
            (static_cast<u64>(y & 0xFFFFu) << 16) | (static_cast<u64>(z & 0xFFFFu) << 32);
@@ -221,11 +224,18 @@ __host__ __device__ __forceinline__ u64 slot_hash(u64 pk) {
     if constexpr (BATCH) return cell_hash_batch(pk);
     else return cell_hash_packed(pk);
 }
-// Sort key of a batched particle: scene in the top bits, the low 48 bits of
-// the reference's Morton key below (identical order inside a scene).
-__host__ __device__ __forceinline__ u64 batch_key(u32 scene, u64 morton) {
-    return (static_cast<u64>(scene) << 48) | (morton & 0xFFFFFFFFFFFFull);
+// Sort key of a batched particle: the scene id in bits 48..62 and, below, the
+// Morton key of the cell coordinates offset by 2^15 (16 bits per axis). For
+// cells in [-2^15, 2^15) it orders the particles of a scene exactly as the
+// reference's 63-bit key of c + 2^20 does: bits 15..19 of c + 2^20 repeat the
+// inverse of its bit 20 (the sign), which bit 15 of c + 2^15 carries, so the
+// first differing bit of two keys sits at the same place in both. The stable
+// sort therefore gives every scene the permutation of its own single step.
+__host__ __device__ __forceinline__ u64 batch_key(u32 scene, int3 c) {
+    return (static_cast<u64>(scene) << 48) | part_by_3(static_cast<u32>(c.x + 32768)) |
+           (part_by_3(static_cast<u32>(c.y + 32768)) << 1) | (part_by_3(static_cast<u32>(c.z + 32768)) << 2);
 }
+constexpr int BATCH_CELL_LIMIT = 32768;   // batched cell coordinates lie in [-limit, limit)
 
 // Linear-probed lookup (find_cell_in_table, common.cuh:89-102). table_size is
 // a power of two so `% T` is a mask; the probe is bounded by T.

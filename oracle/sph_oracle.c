@@ -24,8 +24,9 @@
  *   state metrics          src/cuda/SPH/sph.cu:180-197
  *
  * Neighbour predicate: j != i and |x_i - x_j|^2 <= h^2 with the squared
- * distance rounded as fmaf(dz,dz,fmaf(dy,dy,dx*dx)) in float — the same
- * rounding the CUDA path uses — so neighbour sets compare bit-exactly.
+ * distance rounded as fmaf(dz,dz,fmaf(dx,dx,dy*dy)) in float: the order nvcc
+ * contracts the reference's dot(r, r) = x*x + y*y + z*z into (math.cuh:54-56),
+ * which the CUDA path uses too, so neighbour sets compare bit-exactly.
  */
 #include <math.h>
 #include <stdint.h>
@@ -156,7 +157,7 @@ u32 oracle_cell_ranges(const float* spos, u32 n, float cs, u64* keys_out, u32* s
 /* ---------------------------------------------------------- SPH formulas -- */
 static float dist2f(const float* a, const float* b) {
     const float dx = a[0] - b[0], dy = a[1] - b[1], dz = a[2] - b[2];
-    return fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+    return fmaf(dz, dz, fmaf(dx, dx, dy * dy));
 }
 
 typedef struct {

@@ -108,6 +108,17 @@ def test_external_forces(force):
     check_step(p, bx, pos, np.zeros_like(pos), None, 0.01)
 
 
+def test_neighbour_pair_at_the_support_radius():
+    """A pair whose |r| is within one ulp of h (observed in the reference's own
+    run of the tilting box): neighbours for the reference, so for the CUDA
+    path and the oracle too."""
+    from test_oracle_cpu import edge_pair_scene
+
+    p, bx, pos = edge_pair_scene()
+    got, ref = check_step(p, bx, pos, np.zeros_like(pos), None, 5e-4)
+    assert list(got["neighbors"][0]) == [1, 1]
+
+
 @pytest.mark.parametrize("n", [1, 2, 33, 100])
 def test_tiny_scenes(n):
     p, bx, pos, bpos = dam_break_scene(dims=(6, 6, 6))

@@ -96,6 +96,28 @@ def test_neighbor_sets_against_brute_force():
         assert clear_in <= got and not (got & clear_out)
 
 
+# Two particles of the 1,048,576-particle tilting box at step 6 of the
+# reference's own run, |r| within one ulp of h = 0.016: the reference's
+# kernels (dot(r, r) contracted to fma(z, z, fma(x, x, y*y))) count them as
+# neighbours; the order fma(z, z, fma(y, y, x*x)) would not.
+EDGE_PAIR = ((-0.043888334184885025, 0.30357417464256287, -0.3445073962211609),
+             (-0.044758860021829605, 0.3195130228996277, -0.3434140682220459))
+
+
+def edge_pair_scene():
+    p = wcsph.default_params(particle_radius=0.004, max_time_step=5e-4, cfl_factor=0.0)
+    pos = np.zeros((2, 4), np.float32)
+    pos[:, :3] = np.array(EDGE_PAIR, np.float32)
+    pos[:, 3] = 1.0
+    return p, wcsph.box((-1, -0.5, -0.5), (1, 0.5, 0.5)), pos
+
+
+def test_neighbour_predicate_rounds_like_the_reference():
+    p, bx, pos = edge_pair_scene()
+    r = oracle.step(p, bx, pos, np.zeros_like(pos), None, None, delta=5e-4, nbr_cap=16)
+    assert list(r.nbr_counts) == [1, 1]
+
+
 def test_metrics_known_answer():
     p = wcsph.default_params()
     vel = np.zeros((4, 4), np.float32)
