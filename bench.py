@@ -299,19 +299,25 @@ def run_ours(args, world, rank, local, dist):
     return line
 
 
-def bench_batched(args, n_scenes: int = 256, steps: int = 20):
-    """Ensemble of 256 scenes (log-uniform 2048..65536 particles): one batched
-    simulator vs the same scenes stepped one after another."""
+def bench_batched(args, n_scenes: int = 256, steps: int = 500):
+    """Ensemble of 256 scenes (log-uniform 2048..65536 particles), the 500
+    fixed steps of the workload: one persistent cooperative launch for all
+    steps, the per-stage launches (one graph per step), and the same scenes
+    stepped one after another through the single-scene path."""
     import wcsph
 
     pres = [wcsph.preset_ensemble(args.seed + 1, k) for k in range(n_scenes)]
     total = sum(p.info.fluid_n for p in pres)
     specs = [wcsph.BatchSceneSpec(fluid_pos=s.pos, box=s.box, gravity=tuple(s.params.gravity),
                                   viscosity=s.params.viscosity, boundary_pos=s.bpos) for s in pres]
-    b = wcsph.BatchSimulator(pres[0].params, specs)
-    b.step_n(3, 1e-3)
-    ms_b = b.time_steps(steps, 1e-3)
-    b.close()
+    out = {"scenes": n_scenes, "particles": total, "steps": steps, "unit": METRIC}
+    for mode, persistent in (("persistent", True), ("per_stage", False)):
+        b = wcsph.BatchSimulator(pres[0].params, specs)
+        b.set_persistent(persistent)
+        b.step_n(3, 1e-3)
+        ms = b.time_steps(steps, 1e-3)
+        b.close()
+        out[mode] = total * steps / (ms * 1e-3)
     sims = [s.simulator() for s in pres]
     for sim in sims:
         sim.step_n(3, 1e-3)
@@ -323,11 +329,11 @@ def bench_batched(args, n_scenes: int = 256, steps: int = 20):
     seq_s = time.perf_counter() - t0
     for sim in sims:
         sim.close()
-    vb = total * steps / (ms_b * 1e-3)
-    vs = total * steps / seq_s
-    return {"scenes": n_scenes, "particles": total, "steps": steps, "value": vb, "unit": METRIC,
-            "sequential_value": vs, "gain": vb / vs, "launches_per_step_batched": 14,
-            "launches_per_step_sequential": 14 * n_scenes}
+    out["value"] = out["persistent"]
+    out["sequential_value"] = total * steps / seq_s
+    out["gain"] = out["value"] / out["sequential_value"]
+    out["launches"] = {"persistent": 1, "per_stage": 14 * steps, "sequential": 14 * n_scenes * steps}
+    return out
 
 
 def bench_rollout():

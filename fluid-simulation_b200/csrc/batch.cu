@@ -6,10 +6,16 @@
 // keeps every scene contiguous and, inside a scene, reproduces the
 // reference's Morton order for that scene alone. Cells are hashed by
 // (scene, cell) so neighbourhoods never cross scenes; the integrate pass
-// reads each scene's box, gravity and viscosity from a per-scene table. Every
-// stage is one launch over all scenes and the whole step is replayed from a
-// captured CUDA graph. The time step is fixed (CFL off), as in the
-// ensemble workload.
+// reads each scene's box, gravity and viscosity from a per-scene table. The
+// time step is fixed (CFL off), as in the ensemble workload.
+//
+// Two ways to run k steps, with identical results:
+//  * persistent (default): one cooperative launch of batch_persistent.cu
+//    advances every scene k steps, its phases separated by grid barriers; the
+//    launch is captured in a CUDA graph (or issued directly where the driver
+//    does not capture cooperative launches);
+//  * per stage: one launch per stage and step (keys, sort plan, 8 digit
+//    passes, reorder, 3 passes), the step captured in a CUDA graph.
 #include <algorithm>
 #include <bit>
 #include <cmath>
@@ -25,30 +31,33 @@
 namespace wcsph {
 
 namespace {
-__global__ void batch_metrics_kernel(const float4* __restrict__ vel, const u32* __restrict__ scene, u32 n,
-                                     float* __restrict__ sums /* [S][2] */) {
-    const u32 i = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool valid = i < n;
-    const u32 s = valid ? scene[i] : 0xFFFFFFFFu;
-    float a = 0.f, b = 0.f;
-    if (valid) {
+// Per-scene mean |v| and sum |v|^2 of the state: block k reduces scene k's
+// contiguous range in a fixed order (double accumulators, fixed tree), so the
+// metrics do not depend on scheduling.
+__global__ void batch_metrics_kernel(const float4* __restrict__ vel, const u32* __restrict__ offsets,
+                                     double* __restrict__ sums /* [S][2] */) {
+    __shared__ double s1[256], s2[256];
+    const u32 k = blockIdx.x;
+    double a = 0.0, b = 0.0;
+    for (u32 i = offsets[k] + threadIdx.x; i < offsets[k + 1]; i += blockDim.x) {
         const float4 v = vel[i];
-        b = dot3(v, v);
-        a = sqrtf(b);
+        const float d = dot3(v, v);
+        a += static_cast<double>(sqrtf(d));
+        b += static_cast<double>(d);
     }
-    // aggregate lanes of the same scene (sorted order: usually one per warp)
-    const u32 peers = __match_any_sync(0xffffffffu, s);
-    const u32 lane = threadIdx.x & 31u;
-    const u32 leader = __ffs(peers) - 1;
-    float ta = 0.f, tb = 0.f;
-    for (u32 m = peers; m; m &= m - 1) {
-        const u32 src = __ffs(m) - 1;
-        ta += __shfl_sync(peers, a, src);
-        tb += __shfl_sync(peers, b, src);
+    s1[threadIdx.x] = a;
+    s2[threadIdx.x] = b;
+    __syncthreads();
+    for (u32 o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) {
+            s1[threadIdx.x] += s1[threadIdx.x + o];
+            s2[threadIdx.x] += s2[threadIdx.x + o];
+        }
+        __syncthreads();
     }
-    if (valid && lane == leader) {
-        atomicAdd(&sums[2 * s], ta);
-        atomicAdd(&sums[2 * s + 1], tb);
+    if (threadIdx.x == 0) {
+        sums[2 * k] = s1[0];
+        sums[2 * k + 1] = s2[0];
     }
 }
 }  // namespace
@@ -60,6 +69,7 @@ struct BatchSim {
     int device = 0;
     u32 n = 0, nb = 0, S = 0;
     std::vector<u32> offsets, counts;   // fluid ranges per scene
+    std::vector<u32> scene_first;       // offsets plus the total (uploaded to scene_offsets)
     float metric_mass = 0.f;
 
     DevBuf<float4> pos_a, pos_b, vel_a, vel_b;
@@ -71,7 +81,17 @@ struct BatchSim {
     DevBuf<u32> cstart, cend, mask;
     DevBuf<u32> nbr, nbr_cnt;          // neighbour lists, nbr_width slots per particle
     u32 table_size = 0;
-    DevBuf<float> rho, prs, partials, metric_sums;
+    DevBuf<float> rho, prs, partials;
+    DevBuf<double> metric_sums;
+    DevBuf<u32> scene_offsets;          // [S + 1] first particle of each scene (device copy of offsets)
+    DevBuf<u32> barrier;                // persistent kernel: grid-barrier arrivals and generation
+    bool persistent = true;
+    u32 p_blocks = 0;
+    size_t p_smem = 0;
+    cudaGraphExec_t pgraph = nullptr;   // persistent launch of pgraph_steps steps
+    float pgraph_delta = -1.f;
+    int pgraph_steps = 0;
+    bool coop_capture = true;           // the driver captures cooperative launches
     DevBuf<u32> group_done;
     DevBuf<double> group_partials;
     DevBuf<float4> recf, recs;
@@ -92,6 +112,7 @@ struct BatchSim {
 
     ~BatchSim() {
         if (graph) cudaGraphExecDestroy(graph);
+        if (pgraph) cudaGraphExecDestroy(pgraph);
         if (stream) {
             cudaStreamSynchronize(stream);
             cudaStreamDestroy(stream);
@@ -114,6 +135,7 @@ struct BatchSim {
         a.mask_words = static_cast<u32>(mask_words);
         a.chunk = n < (1u << 18) ? 8u : 16u;
         a.nbr = nbr_width > 0 ? nbr.ptr : nullptr;
+        a.pair_cells = a.nbr != nullptr ? 1u : 0u;
         a.nbr_cnt = nbr_cnt.ptr;
         a.nbr_width = static_cast<u32>(nbr_width);
         a.rho = rho.ptr; a.prs = prs.ptr;
@@ -153,7 +175,74 @@ struct BatchSim {
         launch_pass(PASS_SURFACE, dp, a, stream, 2, true);
     }
 
+    PersistentStep persistent_args(float delta, int steps) {
+        PersistentStep ps{};
+        ps.P = dp;
+        ps.a = args(delta);
+        ps.pos_state = pos_a.ptr;
+        ps.vel_state = vel_a.ptr;
+        ps.scene_state = scene_a.ptr;
+        for (int i = 0; i < 3; ++i) { ps.keys[i] = keys[i].ptr; ps.vals[i] = vals[i].ptr; }
+        ps.hist = hist.ptr;
+        ps.offsets = offs.ptr;
+        ps.lookback = lookback.ptr;
+        ps.tiles = sort_tiles(n);
+        ps.perm = perm.ptr;
+        ps.table = table.ptr;
+        ps.table_size = table_size;
+        ps.cs = dp.cell_size;
+        ps.barrier = barrier.ptr;
+        ps.steps = steps;
+        ps.spin_limit = LB_SPIN_LIMIT;
+        ps.barrier_limit = 1u << 24;   // polls 64 ns apart: about a second
+        return ps;
+    }
+
+    // Captures the cooperative launch of k steps into a graph (once per
+    // (delta, k)); where the driver refuses, later calls launch directly.
+    void prepare_persistent(int k, float delta) {
+        if (k <= 0) return;
+        if (p_blocks == 0) persistent_grid(args(delta), device, &p_blocks, &p_smem);
+        const PersistentStep ps = persistent_args(delta, k);
+        if (coop_capture && (!pgraph || pgraph_delta != delta || pgraph_steps != k)) {
+            if (pgraph) cudaGraphExecDestroy(pgraph);
+            pgraph = nullptr;
+            cudaGraph_t g = nullptr;
+            WCSPH_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+            bool launched = true;
+            try {
+                launch_persistent(ps, p_blocks, p_smem, stream);
+            } catch (const Error&) {
+                launched = false;
+            }
+            const cudaError_t ec = cudaStreamEndCapture(stream, &g);
+            cudaError_t ei = cudaErrorUnknown;
+            if (launched && ec == cudaSuccess && g) ei = cudaGraphInstantiate(&pgraph, g, 0);
+            if (g) cudaGraphDestroy(g);
+            if (ei != cudaSuccess) {   // no capture of cooperative launches: launch directly from now on
+                pgraph = nullptr;
+                coop_capture = false;
+                cudaGetLastError();
+            } else {
+                pgraph_delta = delta;
+                pgraph_steps = k;
+            }
+        }
+    }
+
+    // k steps in one cooperative launch (graph replay when captured)
+    void persistent_steps(int k, float delta) {
+        if (k <= 0) return;
+        prepare_persistent(k, delta);
+        if (pgraph && pgraph_delta == delta && pgraph_steps == k) WCSPH_CUDA(cudaGraphLaunch(pgraph, stream));
+        else launch_persistent(persistent_args(delta, k), p_blocks, p_smem, stream);
+    }
+
     void step_n(int k, float delta) {
+        if (persistent) {
+            persistent_steps(k, delta);
+            return;
+        }
         if (!graph || graph_delta != delta) {
             if (graph) cudaGraphExecDestroy(graph);
             graph = nullptr;
@@ -183,6 +272,8 @@ struct BatchSim {
             WCSPH_CUDA(cudaMemset(&st.ptr->error_flags, 0, sizeof(u32)));
             if (flags & ERR_HASH_FULL) throw Error(WCSPH_ERR_HASH_FULL, "spatial hash table is full");
             if (flags & ERR_LOOKBACK_TIMEOUT) throw Error(WCSPH_ERR_DEVICE_TIMEOUT, "radix sort look-back timed out");
+            if (flags & ERR_BARRIER_TIMEOUT)
+                throw Error(WCSPH_ERR_DEVICE_TIMEOUT, "persistent ensemble kernel: grid barrier timed out");
             throw Error(WCSPH_ERR_NEIGHBOR_OVERFLOW, "boundary candidate cells exceed capacity");
         }
     }
@@ -204,8 +295,9 @@ static void build_batch(BatchSim& B, const wcsph_params& p, const wcsph_batch_sc
     B.metric_mass = metric_mass(p);
     B.S = S;
     const float cs = B.dp.cell_size;
-    // scenes must stay inside one 65536-cell window per axis starting at cell 0
-    const double lim = 65535.0 * cs;
+    // batched cell coordinates must lie in [-2^15, 2^15) (16-bit batch keys),
+    // with a margin for the neighbour cells of the outermost particles
+    const double lim = static_cast<double>(BATCH_CELL_LIMIT - 4) * cs;
     std::vector<float> pos, vel, bp;
     std::vector<u32> sid, bsid;
     std::vector<DevScene> ds(S);
@@ -220,9 +312,17 @@ static void build_batch(BatchSim& B, const wcsph_params& p, const wcsph_batch_sc
     vel.reserve(4 * total);
     for (u32 k = 0; k < S; ++k) {
         const wcsph_batch_scene& s = sc[k];
-        for (int d = 0; d < 3; ++d) {
-            if (!(s.box.min[d] >= 0.f) || !(s.box.max[d] < lim))
-                throw Error(WCSPH_ERR_NOT_SUPPORTED, "batched scene boxes must lie in [0, 65535 cells) per axis");
+        // the box's corners in world space (the model matrix of its frame)
+        for (int c = 0; c < 8; ++c) {
+            const float m[3] = {(c & 1) ? s.box.max[0] : s.box.min[0], (c & 2) ? s.box.max[1] : s.box.min[1],
+                                (c & 4) ? s.box.max[2] : s.box.min[2]};
+            for (int d = 0; d < 3; ++d) {
+                const double w = static_cast<double>(s.box.model[d]) * m[0] + s.box.model[4 + d] * m[1] +
+                                 s.box.model[8 + d] * m[2] + s.box.model[12 + d];
+                if (!(std::fabs(w) < lim))
+                    throw Error(WCSPH_ERR_NOT_SUPPORTED,
+                                "batched scene boxes must lie within 32,764 cells of the origin per axis");
+            }
         }
         B.offsets.push_back(static_cast<u32>(pos.size() / 4));
         B.counts.push_back(s.fluid_n);
@@ -242,8 +342,8 @@ static void build_batch(BatchSim& B, const wcsph_params& p, const wcsph_batch_sc
     }
     for (size_t i = 0; i < pos.size() / 4; ++i)
         for (int d = 0; d < 3; ++d)
-            if (!(pos[4 * i + d] >= 0.f) || !(pos[4 * i + d] < lim))
-                throw Error(WCSPH_ERR_NOT_SUPPORTED, "batched particles must lie in [0, 65535 cells) per axis");
+            if (!(std::fabs(static_cast<double>(pos[4 * i + d])) < lim))
+                throw Error(WCSPH_ERR_NOT_SUPPORTED, "batched particles must lie within 32,764 cells of the origin per axis");
     B.n = static_cast<u32>(total);
     B.nb = static_cast<u32>(btotal);
     const size_t n = B.n;
@@ -267,6 +367,13 @@ static void build_batch(BatchSim& B, const wcsph_params& p, const wcsph_batch_sc
     B.group_partials.alloc(2ull * (pass_max_warps(B.n) / 32u + 1u));
     WCSPH_CUDA(cudaMemsetAsync(B.group_done.ptr, 0, B.group_done.bytes(), B.stream));
     B.metric_sums.alloc(2ull * S);
+    B.scene_offsets.alloc(S + 1ull);
+    B.scene_first = B.offsets;
+    B.scene_first.push_back(B.n);
+    WCSPH_CUDA(cudaMemcpyAsync(B.scene_offsets.ptr, B.scene_first.data(), sizeof(u32) * (S + 1ull),
+                               cudaMemcpyHostToDevice, B.stream));
+    B.barrier.alloc(2);
+    WCSPH_CUDA(cudaMemsetAsync(B.barrier.ptr, 0, B.barrier.bytes(), B.stream));
     B.st.alloc(1);
     B.scenes.alloc(S);
     cudaStream_t s = B.stream;
@@ -363,6 +470,14 @@ int wcsph_batch_destroy(wcsph_batch* b) {
     return WCSPH_OK;
 }
 
+int wcsph_batch_set_persistent(wcsph_batch* b, int enable) {
+    if (!b) return WCSPH_ERR_INVALID_ARGUMENT;
+    return bguard(b, [&] {
+        WCSPH_CUDA(cudaStreamSynchronize(b->sim.stream));
+        b->sim.persistent = enable != 0;
+    });
+}
+
 int wcsph_batch_step_n(wcsph_batch* b, int n, float delta) {
     if (!b || n < 0) return WCSPH_ERR_INVALID_ARGUMENT;
     return bguard(b, [&] { b->sim.step_n(n, delta); });
@@ -371,8 +486,12 @@ int wcsph_batch_step_n(wcsph_batch* b, int n, float delta) {
 int wcsph_batch_time_steps(wcsph_batch* b, int n, float delta, float* ms_out) {
     if (!b || n < 0 || !ms_out) return WCSPH_ERR_INVALID_ARGUMENT;
     return bguard(b, [&] {
-        b->sim.step_n(0, delta);
-        if (!b->sim.graph || b->sim.graph_delta != delta) b->sim.step_n(1, delta);
+        // graphs and launch set-up happen before the timed region
+        if (b->sim.persistent) {
+            b->sim.prepare_persistent(n, delta);
+        } else if (!b->sim.graph || b->sim.graph_delta != delta) {
+            b->sim.step_n(1, delta);
+        }
         cudaEvent_t e0, e1;
         WCSPH_CUDA(cudaEventCreate(&e0));
         WCSPH_CUDA(cudaEventCreate(&e1));
@@ -408,17 +527,15 @@ int wcsph_batch_metrics(wcsph_batch* b, float* mean_speed, float* ke) {
     if (!b) return WCSPH_ERR_INVALID_ARGUMENT;
     return bguard(b, [&] {
         wcsph::BatchSim& B = b->sim;
-        WCSPH_CUDA(cudaMemsetAsync(B.metric_sums.ptr, 0, B.metric_sums.bytes(), B.stream));
-        wcsph::batch_metrics_kernel<<<(B.n + 255) / 256, 256, 0, B.stream>>>(B.vel_a.ptr, B.scene_a.ptr, B.n,
-                                                                            B.metric_sums.ptr);
+        wcsph::batch_metrics_kernel<<<B.S, 256, 0, B.stream>>>(B.vel_a.ptr, B.scene_offsets.ptr, B.metric_sums.ptr);
         WCSPH_CUDA(cudaGetLastError());
-        std::vector<float> sums(2ull * B.S);
-        WCSPH_CUDA(cudaMemcpyAsync(sums.data(), B.metric_sums.ptr, sizeof(float) * sums.size(),
+        std::vector<double> sums(2ull * B.S);
+        WCSPH_CUDA(cudaMemcpyAsync(sums.data(), B.metric_sums.ptr, sizeof(double) * sums.size(),
                                    cudaMemcpyDeviceToHost, B.stream));
         B.check_errors();
         for (uint32_t k = 0; k < B.S; ++k) {
-            if (mean_speed) mean_speed[k] = sums[2 * k] / static_cast<float>(B.counts[k]);
-            if (ke) ke[k] = 0.5f * B.metric_mass * sums[2 * k + 1];
+            if (mean_speed) mean_speed[k] = static_cast<float>(sums[2 * k] / static_cast<double>(B.counts[k]));
+            if (ke) ke[k] = static_cast<float>(0.5 * static_cast<double>(B.metric_mass) * sums[2 * k + 1]);
         }
     });
 }

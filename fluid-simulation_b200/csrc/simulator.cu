@@ -291,6 +291,8 @@ TravArgs CUDASPHSimulator::trav_args(float delta) {
     a.mask_words = static_cast<u32>(cfg_.mask_words);
     a.chunk = effective_chunk(cfg_, n_);
     a.nbr = nbr_width_ > 0 ? nbr_.ptr : nullptr;
+    a.pair_cells = a.nbr != nullptr ? 1u : 0u;   // the lists replace the kept bit matrix
+    a.matrix_valid = 0u;
     a.nbr_cnt = nbr_cnt_.ptr;
     a.nbr_width = nbr_width_;
     a.rho = rho_.ptr; a.prs = prs_.ptr;
@@ -339,6 +341,7 @@ TravArgs CUDASPHSimulator::fixed_args(float dt) {
     a.cfl_factor = 0.f;
     a.max_dt = dt;
     a.min_dt = dt;
+    a.pair_cells = 0u;   // the adjoint passes walk each step's kept bit matrix
     return a;
 }
 

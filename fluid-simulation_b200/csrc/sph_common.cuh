@@ -300,6 +300,7 @@ enum : u32 {
     ERR_HASH_FULL = 1u,
     ERR_LOOKBACK_TIMEOUT = 2u,
     ERR_CAND_OVERFLOW = 4u,
+    ERR_BARRIER_TIMEOUT = 8u,   // a grid barrier of the persistent ensemble kernel waited too long
 };
 
 }  // namespace wcsph

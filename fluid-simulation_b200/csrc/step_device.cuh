@@ -56,6 +56,14 @@ constexpr u32 HOME_BLOCK = 32;   // home particles (bit-matrix rows) handled tog
 constexpr u32 SEG_SLOTS = 64;    // segment partials, slot = lane + row (both < 32)
 constexpr u32 NO_HOME = 0xFFFFFFFFu;   // home rows not among the staged candidates
 
+// Candidate index of home row k of a home block: rows [0, split) are staged
+// at c1 + k, later rows at c2 + (k - split) (the second cell of an x-pair);
+// c1 == NO_HOME: the home rows are not staged (read from global memory).
+struct HomeMap {
+    u32 split, c1, c2;
+    __device__ __forceinline__ u32 cand(u32 k) const { return k < split ? c1 + k : c2 + (k - split); }
+};
+
 
 __device__ __forceinline__ u32 lane_id() { return threadIdx.x & 31u; }
 
@@ -93,10 +101,11 @@ struct KindCfg {
                               : (KIND == PASS_SURFACE || KIND == PASS_ADJ_DENSITY) ? 3 : 1;
     static constexpr int nfb = KIND == PASS_ADJ_FORCE ? 4 : (KIND == PASS_DENSITY ? 1 : 3);
     // resident warps per SM the register allocation must allow (32 -> 64 registers,
-    // 24 -> 80, 16 -> 128): the force pass spills below 80 registers, the
-    // adjoint force pass below 128
-    static constexpr int min_warps =
-        (KIND == PASS_DENSITY || KIND == PASS_SURFACE) ? 32 : (KIND == PASS_ADJ_FORCE ? 16 : 24);
+    // 28 -> 72, 24 -> 80, 16 -> 128): the density pass spills a little at 72
+    // registers, which costs less than fewer resident warps at 80; the force
+    // pass below 80, the adjoint force pass below 128
+    static constexpr int min_warps = KIND == PASS_DENSITY ? 28
+                                     : KIND == PASS_SURFACE ? 32 : (KIND == PASS_ADJ_FORCE ? 16 : 24);
 };
 
 __host__ __device__ constexpr size_t align16(size_t b) { return (b + 15) & ~static_cast<size_t>(15); }
@@ -136,8 +145,10 @@ __host__ __device__ __forceinline__ size_t warp_smem_bytes(u32 cap, u32 ncell, b
     unsigned char* sp = C::soa ? take(8ull * pair_slot(cap / 2)) : nullptr;
     unsigned char* cand = C::stage_j ? take(4ull * cap) : nullptr;
     unsigned char* cq = C::stage_q ? take(cap) : nullptr;
-    unsigned char* rstart = take(4ull * (ncell + 3));
-    unsigned char* rpref = take(4ull * (ncell + 3));
+    // density: room for the 36-cell union of an x-pair of cells (R = 1)
+    const u32 nrange = (KIND == PASS_DENSITY && ncell < 36u) ? 36u : ncell;
+    unsigned char* rstart = take(4ull * (nrange + 3));
+    unsigned char* rpref = take(4ull * (nrange + 3));
     unsigned char *bcand = nullptr, *bstart = nullptr, *bpref = nullptr;
     if (C::boundary && with_boundary) {   // only scenes with boundary particles
         bcand = take(4ull * BCAND_CAP);
@@ -250,15 +261,20 @@ __device__ __forceinline__ void stage(const WarpView<KIND>& S, const TravArgs& a
     const u32 lane = lane_id();
     const u32 c1 = c0 + len;
     for (u32 qb = 0; qb < ncell; qb += 32) {
-        const u32 q = qb + lane;
+        // a last round of fewer than 32 cells (the 36-cell union of an x-pair)
+        // spreads each cell over 32 / cells lanes
+        const u32 rem = min(32u, ncell - qb);
+        const u32 lpc = rem == 32u ? 1u : 32u / rem;
+        const u32 q = qb + lane / lpc;
+        const u32 sub = lane - (lane / lpc) * lpc;
         u32 lo = 0, hi = 0, src = 0;
-        if (q < ncell) {
+        if (lane / lpc < rem) {
             const u32 b = S.rpref[q], e = S.rpref[q + 1];
             lo = max(b, c0);
             hi = min(e, c1);
             src = S.rstart[q] + (lo - b);
         }
-        for (u32 t = 0; lo + t < hi; ++t) {
+        for (u32 t = sub; lo + t < hi; t += lpc) {
             const u32 j = src + t;
             const u32 ml = lo + t - c0;
             if constexpr (KindCfg<KIND>::stage_j) S.cand[ml] = j;
@@ -617,12 +633,12 @@ __device__ __forceinline__ u32 fluid_pair_run(const WarpView<KIND>& S, const Dev
 }
 
 // Position of home row k of the density pass: from the staged candidates
-// (home_m0 = candidate index of row 0) when they hold the home cell, else
+// (hm maps rows to candidate indices) when they hold the home cells, else
 // from global memory.
-__device__ __forceinline__ float4 home_x(const WarpView<PASS_DENSITY>& S, const TravArgs& a, u32 i0, u32 home_m0,
+__device__ __forceinline__ float4 home_x(const WarpView<PASS_DENSITY>& S, const TravArgs& a, u32 i0, HomeMap hm,
                                          u32 k) {
-    if (home_m0 != NO_HOME) {
-        const u32 m = home_m0 + k;
+    if (hm.c1 != NO_HOME) {
+        const u32 m = hm.cand(k);
         const float* f = reinterpret_cast<const float*>(S.sp + pair_slot(m >> 1)) + (m & 1u);
         return make_float4(f[0], f[2], f[4], 0.f);
     }
@@ -637,12 +653,12 @@ __device__ __forceinline__ float4 home_x(const WarpView<PASS_DENSITY>& S, const 
 template <int KIND, bool SHARED_BITS = false>
 __device__ __forceinline__ u32 fluid_hit_run(const WarpView<KIND>& S, const DevParams& P, const TravArgs& a,
                                              const u32* __restrict__ bits, u32 nh, u32 M, u32 i0, u32& lo,
-                                             u32& hi, bool lists = false, u32 home_m0 = NO_HOME) {
+                                             u32& hi, bool lists = false, HomeMap hm = HomeMap{32u, NO_HOME, 0u}) {
     auto home = [&](u32 k) -> HomeData {
         if constexpr (KIND == PASS_DENSITY) {
-            if (home_m0 != NO_HOME) {
+            if (hm.c1 != NO_HOME) {
                 HomeData H;
-                H.x = home_x(S, a, i0, home_m0, k);
+                H.x = home_x(S, a, i0, hm, k);
                 return H;
             }
         }
@@ -739,8 +755,12 @@ __device__ __forceinline__ u32 fluid_hit_run(const WarpView<KIND>& S, const DevP
 // unrolled, each tested in packed FP32 with the rounding of dist2()
 // (x_i - x_j is formed as fma(x_j, -1, x_i), the same single rounding).
 // The home particle's own bit is set here and cleared by the caller.
+// Row windows: rows [0, hm.split) keep candidates [0, win_a) only, later rows
+// [win_b, 32 wpr) only (the two cells of an x-pair, each restricted to its own
+// 27 neighbour cells; a single cell passes win_a = 32 wpr).
 __device__ __forceinline__ void density_test_words(const WarpView<PASS_DENSITY>& S, const DevParams& P,
-                                                   const TravArgs& a, u32 nh, u32 wpr, u32 i0, u32 home_m0) {
+                                                   const TravArgs& a, u32 nh, u32 wpr, u32 i0, HomeMap hm,
+                                                   u32 win_a, u32 win_b) {
     const u32 nwords = nh * wpr;
     const float2 neg = make_float2(-1.f, -1.f);
     // w / wpr as a multiply-high: exact for w < 2^32 / wpr^2 (here w < 32 * 16)
@@ -748,7 +768,7 @@ __device__ __forceinline__ void density_test_words(const WarpView<PASS_DENSITY>&
     for (u32 w = lane_id(); w < nwords; w += 32) {
         const u32 k = wpr == 1u ? w : __umulhi(w, inv);
         const u32 wi = w - k * wpr;
-        const float4 h = home_x(S, a, i0, home_m0, k);
+        const float4 h = home_x(S, a, i0, hm, k);
         const float2 X = make_float2(h.x, h.x), Y = make_float2(h.y, h.y), Z = make_float2(h.z, h.z);
         const float2* base = S.sp + pair_slot(wi * 16u);
         u32 bits = 0;
@@ -760,6 +780,11 @@ __device__ __forceinline__ void density_test_words(const WarpView<PASS_DENSITY>&
             const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dx, dx, __fmul2_rn(dy, dy)));
             bits |= (r2.x <= P.h2 ? 1u << (2 * t) : 0u) | (r2.y <= P.h2 ? 2u << (2 * t) : 0u);
         }
+        // candidates [lo, hi) of the row's window within this word
+        const u32 lo = k < hm.split ? 0u : win_b, hi = k < hm.split ? win_a : 0xFFFFFFFFu;
+        const u32 w0 = wi << 5;
+        if (lo > w0) bits &= lo >= w0 + 32u ? 0u : FULL << (lo - w0);
+        if (hi < w0 + 32u) bits &= hi <= w0 ? 0u : FULL >> (w0 + 32u - hi);
         S.aux[w] = bits;
     }
     __syncwarp();
@@ -1152,16 +1177,72 @@ __device__ __forceinline__ void cell_pass_chunk(const DevParams& P, const TravAr
                 uy = static_cast<u32>((pk >> 21) & 0x1FFFFFull);
                 uz = static_cast<u32>((pk >> 42) & 0x1FFFFFull);
             }
+            // Density with lists: a cell of even x and the cell of x + 1 after
+            // it (Morton-consecutive, so adjacent in sorted order whenever both
+            // are occupied) form an x-pair, handled whole by the warp of the
+            // first: one lookup of the union of their neighbour cells (4 x 3 x 3,
+            // in the reference's x, y, z order), one staging, and twice the
+            // home rows per walk. The warp of the second cell skips it.
+            bool pair_try = false;
+            if constexpr (KIND == PASS_DENSITY) {
+                if (a.pair_cells && R == 1) {
+                    if (ux & 1u) {
+                        u64 apk;
+                        if constexpr (BATCH) apk = pack_cell_batch(scene, ux - 1u, uy, uz);
+                        else apk = pack_cell(ux - 1u, uy, uz);
+                        if (__shfl_sync(FULL, prev_pk, s) == apk && base + s > 0) continue;
+                    } else {
+                        pair_try = true;
+                    }
+                }
+            }
+            u32 gx = ux;   // x of the cell whose neighbourhood is gathered
+            auto gather = [&](u32 nc) {
+                return gather_ranges<BATCH>(S.rstart, S.rpref, nc, a.fluid, [&](u32 q) {
+                    int dx, dy, dz;
+                    cell_offset(q, R, dx, dy, dz);   // R = 1: q < 36 gives dx in [-1, 2]
+                    if constexpr (BATCH) return pack_cell_batch(scene, gx + dx, uy + dy, uz + dz);
+                    else return pack_cell(gx + dx, uy + dy, uz + dz);
+                });
+            };
+            u32 units = 1;
+            for (u32 unit = 0; unit < units; ++unit) {
             // fluid neighbour cells in the reference's x, y, z nesting order
-            const u32 M = gather_ranges<BATCH>(S.rstart, S.rpref, ncell, a.fluid, [&](u32 q) {
-                int dx, dy, dz;
-                cell_offset(q, R, dx, dy, dz);
-                if constexpr (BATCH) return pack_cell_batch(scene, ux + dx, uy + dy, uz + dz);
-                else return pack_cell(ux + dx, uy + dy, uz + dz);
-            });
-            const u32 home_start = S.rstart[qc];
-            const u32 n_home = S.rpref[qc + 1] - S.rpref[qc];
-            const u32 self_base = S.rpref[qc];   // candidate index of the first home particle
+            u32 M, ncs, home_start, n_home, self_base;
+            bool pair = false;
+            u32 nA = 0, selfB = 0, winA = 0, winB = 0;
+            if (unit == 0) {
+                M = gather(pair_try ? 36u : ncell);
+                ncs = ncell;
+                home_start = S.rstart[qc];
+                n_home = S.rpref[qc + 1] - S.rpref[qc];
+                self_base = S.rpref[qc];   // candidate index of the first home particle
+                if (pair_try) {
+                    // union cells 0..26: the first cell's neighbourhood, 9..35: the second's
+                    nA = n_home;
+                    const u32 nB = S.rpref[23] - S.rpref[22];
+                    const bool second = nB > 0 && S.rstart[22] == home_start + nA;
+                    if (second && ((M + 31u) & ~31u) <= a.mask_words * 32u) {
+                        pair = true;
+                        ncs = 36;
+                        n_home = nA + nB;
+                        selfB = S.rpref[22];
+                        winA = S.rpref[27];
+                        winB = S.rpref[9];
+                    } else {
+                        M = S.rpref[27];   // the first cell alone (its 27 cells lead the union)
+                        if (second) units = 2;
+                    }
+                }
+            } else {
+                // the second cell of a pair whose union exceeds the bit-matrix capacity
+                gx = ux + 1u;
+                M = gather(ncell);
+                ncs = ncell;
+                home_start = S.rstart[qc];
+                n_home = S.rpref[qc + 1] - S.rpref[qc];
+                self_base = S.rpref[qc];
+            }
             const u32 Mrow = (M + 31u) & ~31u;     // bit-matrix row length (whole words)
             const bool masked = Mrow <= cap;
 
@@ -1201,7 +1282,7 @@ __device__ __forceinline__ void cell_pass_chunk(const DevParams& P, const TravAr
                 }
             }
 
-            if (masked) stage<KIND>(S, a, ncell, 0, M);
+            if (masked) stage<KIND>(S, a, ncs, 0, M);
             // the cell's neighbour bit matrix: row k = home particle k, bit m = candidate m
             u32* const cell_bits = a.mask + static_cast<size_t>(home_start) * a.mask_words;
 
@@ -1209,6 +1290,10 @@ __device__ __forceinline__ void cell_pass_chunk(const DevParams& P, const TravAr
                 const u32 nh = min(HOME_BLOCK, n_home - hb);
                 const u32 i0 = home_start + hb;
                 const u32 self0 = self_base + hb;
+                // candidate index of each home row of the block (x-pairs: the
+                // rows of the second cell follow those of the first)
+                const HomeMap hm = pair ? HomeMap{nA > hb ? nA - hb : 0u, self0, selfB + (hb > nA ? hb - nA : 0u)}
+                                        : HomeMap{32u, self0, 0u};
                 const bool act = lane < nh;
                 const u32 i = i0 + (act ? lane : 0u);
                 u32* const blk_bits = cell_bits + (hb >> 5) * Mrow;   // row hb starts at bit hb * Mrow
@@ -1224,7 +1309,7 @@ __device__ __forceinline__ void cell_pass_chunk(const DevParams& P, const TravAr
                     u32 cnt = 0;
                     u32 wpos = 0;
                     if constexpr (KIND == PASS_FILL) wpos = act ? a.offsets[i] : 0u;
-                    if (masked) {
+                    if (masked && a.matrix_valid) {
                         if (act) {
                             const u32 b0 = lane * Mrow, b1 = b0 + Mrow - 1;
                             for (u32 w = b0 >> 5; w <= (b1 >> 5); ++w) {
@@ -1247,7 +1332,7 @@ __device__ __forceinline__ void cell_pass_chunk(const DevParams& P, const TravAr
                         const float4 xi = a.pos[i];
                         for (u32 c0 = 0; c0 < M; c0 += cap) {
                             const u32 len = min(cap, M - c0);
-                            stage<KIND>(S, a, ncell, c0, len);
+                            stage<KIND>(S, a, ncs, c0, len);
                             if (act) {
                                 for (u32 ml = 0; ml < len; ++ml) {
                                     if (c0 + ml != self0 + lane && dist2(xi, S.sa[ml]) <= P.h2) {
@@ -1273,9 +1358,10 @@ __device__ __forceinline__ void cell_pass_chunk(const DevParams& P, const TravAr
                         const u32 wpr = (len + 31u) >> 5;
                         const u32 len32 = wpr << 5;
                         const u32 nwords = nh * wpr;
-                        const u32 home_m0 = keep_bits ? self0 : NO_HOME;   // masked: the home cell is staged
-                        density_test_words(S, P, a, nh, wpr, i0, home_m0);
-                        const u32 self = self0 + lane - c0;   // chunk index of the home particle itself
+                        // masked: the home cells are staged
+                        const HomeMap hmc = keep_bits ? hm : HomeMap{32u, NO_HOME, 0u};
+                        density_test_words(S, P, a, nh, wpr, i0, hmc, pair ? winA : len32, winB);
+                        const u32 self = (keep_bits ? hm.cand(lane) : self0 + lane) - c0;   // the home particle itself
                         if (act && self < len) {
                             const u32 item = lane * len32 + self;
                             atomicAnd(S.aux + (item >> 5), ~(1u << (item & 31u)));
@@ -1283,10 +1369,10 @@ __device__ __forceinline__ void cell_pass_chunk(const DevParams& P, const TravAr
                         __syncwarp();
                         u32 lo, hi;
                         const u32 c = fluid_hit_run<KIND, true>(S, P, a, S.aux, nh, len32, i0, lo, hi,
-                                                                keep_bits && a.nbr != nullptr, home_m0);
+                                                                keep_bits && a.nbr != nullptr, hmc);
                         if (c) combine<NF>(S.part, res, act, lo, hi, c, lane);
                         if (keep_bits && hi - lo <= a.nbr_width) row_cnt = hi - lo;
-                        if (keep_bits)
+                        if (keep_bits && !a.pair_cells)   // kept for the neighbour export and the adjoint
                             for (u32 w = lane; w < nwords; w += 32) blk_bits[w] = S.aux[w];
                         __syncwarp();
                     };
@@ -1295,7 +1381,7 @@ __device__ __forceinline__ void cell_pass_chunk(const DevParams& P, const TravAr
                     } else {
                         for (u32 c0 = 0; c0 < M; c0 += cap) {
                             const u32 len = min(cap, M - c0);
-                            stage<KIND>(S, a, ncell, c0, len);
+                            stage<KIND>(S, a, ncs, c0, len);
                             density_chunk(c0, len, false);
                         }
                     }
@@ -1311,7 +1397,7 @@ __device__ __forceinline__ void cell_pass_chunk(const DevParams& P, const TravAr
                     } else {
                         for (u32 c0 = 0; c0 < M; c0 += cap) {
                             const u32 len = min(cap, M - c0);
-                            stage<KIND>(S, a, ncell, c0, len);
+                            stage<KIND>(S, a, ncs, c0, len);
                             const u32 c = fluid_pair_run<KIND>(S, P, a, nh, len, c0, i0, self0);
                             combine<NF>(S.part, res, act, lane * len, lane * len + len, c, lane);
                         }
@@ -1332,6 +1418,7 @@ __device__ __forceinline__ void cell_pass_chunk(const DevParams& P, const TravAr
                     finish_row<KIND, BATCH>(P, a, i, res, resb, row_cnt, scene, dt, np_dt, red_max, red_speed,
                                             red_speed2);
             }
+            }   // units
         }
     }
 
@@ -1359,6 +1446,56 @@ __device__ __forceinline__ u64 cell_key_of(float4 p, float cs, const u32* scene_
     if constexpr (BATCH) return pack_cell_batch(scene_in[src], offset_coord(c.x), offset_coord(c.y), offset_coord(c.z));
     else return pack_cell(c);
 }
+
+// Reorder + hash build for sorted index i (gather pos/vel into sorted order,
+// cell keys, run starts/ends into the hash; rebuild_n_search.cu:19-34). All 32
+// lanes of a warp must call it together (i >= n for the idle ones).
+template <bool BATCH>
+__device__ __forceinline__ void reorder_cell_item(const float4* __restrict__ pos_in, const float4* __restrict__ vel_in,
+                                                  const u32* __restrict__ v1, const u32* __restrict__ v2,
+                                                  const DevState* st, u32 n, float cs, float4* __restrict__ pos_out,
+                                                  float4* __restrict__ vel_out, u32* __restrict__ perm_out,
+                                                  u64* __restrict__ ckey_out, u64* table, u32* cstart, u32* cend,
+                                                  u32 tmask, DevState* st_err, const u32* __restrict__ scene_in, u32 i) {
+    const u32 lane = threadIdx.x & 31u;
+    const u32 sel = st->sort_sel[8];
+    const u32* perm = sel == 0 ? nullptr : (sel == 1 ? v1 : v2);
+    const bool valid = i < n;
+    u64 pk = 0;
+    if (valid) {
+        const u32 src = perm ? perm[i] : i;
+        const float4 p = pos_in[src];
+        pos_out[i] = p;
+        if (vel_out) vel_out[i] = vel_in[src];
+        perm_out[i] = src;
+        pk = cell_key_of<BATCH>(p, cs, scene_in, src);
+        ckey_out[i] = pk;
+    }
+    u64 prev = __shfl_up_sync(FULL, pk, 1);
+    u64 next = __shfl_down_sync(FULL, pk, 1);
+    if (valid && lane == 0 && i > 0) {
+        const u32 s2 = perm ? perm[i - 1] : i - 1;
+        prev = cell_key_of<BATCH>(pos_in[s2], cs, scene_in, s2);
+    }
+    if (valid && lane == 31 && i + 1 < n) {
+        const u32 s2 = perm ? perm[i + 1] : i + 1;
+        next = cell_key_of<BATCH>(pos_in[s2], cs, scene_in, s2);
+    }
+    if (!valid) return;
+    // rebuild_n_search.cu:19-34: a run of equal cells starts where the key
+    // changes and ends (non-inclusive) at the next change.
+    if (i == 0 || pk != prev) {
+        const u32 slot = hash_insert<BATCH>(table, tmask, pk);
+        if (slot == EMPTY_CELL) atomicOr(&st_err->error_flags, ERR_HASH_FULL);
+        else cstart[slot] = i;
+    }
+    if (i == n - 1 || pk != next) {
+        const u32 slot = hash_insert<BATCH>(table, tmask, pk);
+        if (slot == EMPTY_CELL) atomicOr(&st_err->error_flags, ERR_HASH_FULL);
+        else cend[slot] = i + 1;
+    }
+}
+
 
 }  // namespace
 }  // namespace wcsph

@@ -78,44 +78,8 @@ __global__ void reorder_cells_kernel(const float4* __restrict__ pos_in, const fl
     // a sort whose look-back wait ran out left no permutation: keep the
     // previous sorted state and hash (every later pass returns at once too)
     if (st->error_flags & ERR_LOOKBACK_TIMEOUT) return;
-    const u32 i = blockIdx.x * blockDim.x + threadIdx.x;
-    const u32 lane = threadIdx.x & 31u;
-    const u32 sel = st->sort_sel[8];
-    const u32* perm = sel == 0 ? nullptr : (sel == 1 ? v1 : v2);
-    const bool valid = i < n;
-    u64 pk = 0;
-    if (valid) {
-        const u32 src = perm ? perm[i] : i;
-        const float4 p = pos_in[src];
-        pos_out[i] = p;
-        if (vel_out) vel_out[i] = vel_in[src];
-        perm_out[i] = src;
-        pk = cell_key_of<BATCH>(p, cs, scene_in, src);
-        ckey_out[i] = pk;
-    }
-    u64 prev = __shfl_up_sync(FULL, pk, 1);
-    u64 next = __shfl_down_sync(FULL, pk, 1);
-    if (valid && lane == 0 && i > 0) {
-        const u32 s2 = perm ? perm[i - 1] : i - 1;
-        prev = cell_key_of<BATCH>(pos_in[s2], cs, scene_in, s2);
-    }
-    if (valid && lane == 31 && i + 1 < n) {
-        const u32 s2 = perm ? perm[i + 1] : i + 1;
-        next = cell_key_of<BATCH>(pos_in[s2], cs, scene_in, s2);
-    }
-    if (!valid) return;
-    // rebuild_n_search.cu:19-34: a run of equal cells starts where the key
-    // changes and ends (non-inclusive) at the next change.
-    if (i == 0 || pk != prev) {
-        const u32 slot = hash_insert<BATCH>(table, tmask, pk);
-        if (slot == EMPTY_CELL) atomicOr(&st_err->error_flags, ERR_HASH_FULL);
-        else cstart[slot] = i;
-    }
-    if (i == n - 1 || pk != next) {
-        const u32 slot = hash_insert<BATCH>(table, tmask, pk);
-        if (slot == EMPTY_CELL) atomicOr(&st_err->error_flags, ERR_HASH_FULL);
-        else cend[slot] = i + 1;
-    }
+    reorder_cell_item<BATCH>(pos_in, vel_in, v1, v2, st, n, cs, pos_out, vel_out, perm_out, ckey_out, table, cstart,
+                             cend, tmask, st_err, scene_in, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 __global__ void init_cfl_kernel(const float4* __restrict__ vel, u32 n, DevState* st) {

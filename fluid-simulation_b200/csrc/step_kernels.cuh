@@ -75,6 +75,9 @@ struct TravArgs {
     // neighbour bitmasks
     u32* mask;
     u32 mask_words;           // words per particle (candidate cap = 32*mask_words)
+    u32 pair_cells;           // density with lists: x-pairs of cells share one traversal; the bit
+                              // matrix is then not kept (nothing reads it: the lists carry the sets)
+    u32 matrix_valid;         // neighbour export: the mask buffer holds the last density pass's matrix
     u32 chunk;                // sorted particles per warp chunk: 8, 16 or 32
     // neighbour lists (nullptr: the force and surface passes walk the bit matrix)
     u32* nbr;                 // slot t of particle i at nbr[t * n + i], t < nbr_width, candidate order

@@ -187,6 +187,7 @@ def load_library(path: str | os.PathLike | None = None) -> C.CDLL:
         "wcsph_batch_create": (C.c_int, [C.POINTER(Params), C.POINTER(BatchScene), C.c_uint32, C.c_int,
                                          C.POINTER(vp)]),
         "wcsph_batch_destroy": (C.c_int, [vp]),
+        "wcsph_batch_set_persistent": (C.c_int, [vp, C.c_int]),
         "wcsph_batch_step_n": (C.c_int, [vp, C.c_int, C.c_float]),
         "wcsph_batch_time_steps": (C.c_int, [vp, C.c_int, C.c_float, f]),
         "wcsph_batch_get_state": (C.c_int, [vp, C.c_uint32, f, f]),
@@ -682,6 +683,11 @@ class BatchSimulator:
     def _c(self, st):
         if st != OK:
             raise WcsphError(st, self._lib.wcsph_batch_last_error(self._b).decode())
+
+    def set_persistent(self, enable: bool):
+        """True (default): n steps in one persistent cooperative launch;
+        False: one launch per stage and step (wcsph_batch_set_persistent)."""
+        self._c(self._lib.wcsph_batch_set_persistent(self._b, 1 if enable else 0))
 
     def step_n(self, n, delta):
         self._c(self._lib.wcsph_batch_step_n(self._b, n, delta))

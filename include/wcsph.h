@@ -306,6 +306,13 @@ typedef struct wcsph_batch_scene {
 int wcsph_batch_create(const wcsph_params* params, const wcsph_batch_scene* scenes,
                        uint32_t n_scenes, int device, wcsph_batch** out);
 int wcsph_batch_destroy(wcsph_batch* b);
+/* Chooses how wcsph_batch_step_n / _time_steps run n steps (both give the
+ * same results, bit for bit): enable != 0 (the default) advances every scene
+ * n steps in ONE persistent cooperative launch whose phases are separated by
+ * bounded grid barriers (captured in a CUDA graph where the driver allows);
+ * 0 launches each stage of each step separately from a per-step CUDA graph.
+ * No counterpart in the reference (it has no batched ensembles).          */
+int wcsph_batch_set_persistent(wcsph_batch* b, int enable);
 int wcsph_batch_step_n(wcsph_batch* b, int n, float delta);
 int wcsph_batch_time_steps(wcsph_batch* b, int n, float delta, float* ms_out);
 /* Per-scene state in each scene's current (sorted) order.                  */

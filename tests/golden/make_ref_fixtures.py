@@ -52,9 +52,10 @@ def one(name: str, out_dir: Path):
     print(name, "ok", int(cnt.sum()), "neighbour pairs", flush=True)
 
 
-def trajectory(name: str, out_dir: Path, steps: int, full: set[int]):
-    """The reference's own trajectory of `steps` steps from the scene's initial
-    state, one directory per step: the step's input state (in_pos, in_vel),
+def trajectory(name: str, out_dir: Path, steps: int, full: set[int], skip: int = 0):
+    """The reference's own trajectory of `steps` steps, after `skip` unrecorded
+    steps from the scene's initial state, one directory per recorded step: the
+    step's input state (in_pos, in_vel),
     its sorted keys, permutation, (dt, np_dt), density, pressure and neighbour
     counts; steps in `full` also keep every field and the neighbour lists.
     A moving box is set to the scene's schedule before each step, as bench.py
@@ -69,13 +70,17 @@ def trajectory(name: str, out_dir: Path, steps: int, full: set[int]):
         pre = wcsph.preset(name)
         box_at = pre.box_at if pre.info.moving_box else None
     sim = refpath.RefSim(name, pos, vel, bpos, bx)
-    in_pos, in_vel = pos, vel
+    for k in range(skip):
+        if box_at is not None:
+            sim.set_box(box_at(k + 1))
+        sim.step(delta)
+    in_pos, in_vel = (pos, vel) if skip == 0 else sim.state()
     n = pos.shape[0]
     for k in range(steps):
         d = out_dir / f"step_{k:04d}"
         d.mkdir(parents=True, exist_ok=True)
         if box_at is not None:
-            sim.set_box(box_at(k + 1))
+            sim.set_box(box_at(skip + k + 1))
         sim.step(delta)
         np.save(d / "in_pos.npy", in_pos)
         np.save(d / "in_vel.npy", in_vel)
@@ -111,10 +116,14 @@ def trajectory(name: str, out_dir: Path, steps: int, full: set[int]):
 
 
 def main():
-    # make_ref_fixtures.py [out_dir [scene [--trajectory STEPS [FULL_STEP ...]]]]
+    # make_ref_fixtures.py [out_dir [scene [--trajectory STEPS [--skip N] [FULL_STEP ...]]]]
     out = Path(sys.argv[1]) if len(sys.argv) > 1 else HERE
     if len(sys.argv) > 3 and sys.argv[3] == "--trajectory":
-        trajectory(sys.argv[2], out, int(sys.argv[4]), {int(x) for x in sys.argv[5:]})
+        rest = sys.argv[5:]
+        skip = 0
+        if rest[:1] == ["--skip"]:
+            skip, rest = int(rest[1]), rest[2:]
+        trajectory(sys.argv[2], out, int(sys.argv[4]), {int(x) for x in rest}, skip)
         return
     if len(sys.argv) > 2:
         one(sys.argv[2], out)

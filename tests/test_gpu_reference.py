@@ -82,25 +82,27 @@ def test_cuda_path_matches_reference_kernels(name, tmp_path):
     assert not fails, fails
 
 
-def reference_trajectory(name, steps, full, tmp_path):
+def reference_trajectory(name, steps, full, skip, tmp_path):
     if not refpath.available(name):
         pytest.skip(f"no reference harness for {name}")
     out = tmp_path / f"traj_{name}"
-    subprocess.run([sys.executable, str(GEN), str(out), name, "--trajectory", str(steps), *map(str, full)],
-                   check=True, timeout=1800)
+    subprocess.run([sys.executable, str(GEN), str(out), name, "--trajectory", str(steps), "--skip", str(skip),
+                    *map(str, full)], check=True, timeout=1800)
     return out
 
 
-@pytest.mark.parametrize("name,steps,full", [("mesh_obstacle", 50, (0, 1, 25, 49)),
-                                             ("large_tilting", 10, (0, 9))])
-def test_reference_trajectory_replayed_step_by_step(name, steps, full, tmp_path):
-    """Config 1 (mesh obstacle, CFL 0.4, dt cap 1e-3) for 50 steps and the
-    1,048,576-particle tilting box for 10 steps of its box schedule: at every
+@pytest.mark.parametrize("name,steps,skip,full", [("mesh_obstacle", 50, 450, (0, 1, 25, 49)),
+                                                  ("large_tilting", 10, 0, (0, 9))])
+def test_reference_trajectory_replayed_step_by_step(name, steps, skip, full, tmp_path):
+    """Config 1 (mesh obstacle, CFL 0.4, dt cap 1e-3) for 50 steps from
+    t = 0.45 s, when the collapsing column hits the floor and the sphere at
+    about 4.4 m/s and the CFL rule sets dt, and the 1,048,576-particle tilting
+    box for its first 10 steps of its box schedule: at every
     step the CFL step (dt_p, np_dt), sorted Morton keys, permutation and
     neighbour counts equal the reference's and density is within 1e-5; at
     the `full` steps the neighbour lists are compared in reference order and
     every field is checked."""
-    traj = reference_trajectory(name, steps, full, tmp_path)
+    traj = reference_trajectory(name, steps, full, skip, tmp_path)
     pre = wcsph.preset(name)
     p, delta = pre.params, pre.info.delta
     sim = wcsph.CUDASPHSimulator(p, pre.pos, pre.box, fluid_vel=pre.vel, boundary_pos=pre.bpos)
@@ -112,7 +114,7 @@ def test_reference_trajectory_replayed_step_by_step(name, steps, full, tmp_path)
             in_pos, in_vel = ld("in_pos"), ld("in_vel")
             sim.set_state(in_pos, in_vel)
             if pre.info.moving_box:
-                sim.set_box(pre.box_at(k + 1))
+                sim.set_box(pre.box_at(skip + k + 1))
             sim.update(delta)
             dt = sim.last_dt()
             want_dt = ld("dt")
@@ -143,5 +145,7 @@ def test_reference_trajectory_replayed_step_by_step(name, steps, full, tmp_path)
     finally:
         sim.close()
     if name == "mesh_obstacle":
-        # the run must exercise the CFL rule, not only the dt cap
-        assert min(dts) < float(np.float32(p.max_time_step)), dts
+        # the replayed steps must exercise the CFL rule, not only the dt cap
+        capped = sum(d == float(np.float32(p.max_time_step)) for d in dts)
+        print(f"{name}: dt from {min(dts):.3g} to {max(dts):.3g}, {steps - capped} of {steps} steps set by CFL")
+        assert capped < steps, dts
