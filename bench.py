@@ -44,6 +44,13 @@ PASS_BYTES = {
     "reorder_cells": 4 + 32 + 32 + 8 + 4,
 }
 STEP_BYTES = 400  # algorithmic bytes per fluid particle-step of the reference step structure
+# Algorithmic FP32 work per particle-step of the reference step structure:
+# ~135 FLOP per neighbour pair over density, pressure force and non-pressure
+# force (about 33 neighbours), plus ~9 FLOP per candidate distance test
+# (about 216 candidates in 27 cells) in each of the three passes.
+STEP_FLOP = 135 * 33 + 9 * 216 * 3
+# Nominal FP32 (non-tensor) peak: 148 SMs x 128 FP32 lanes x 2 FLOP x 1.965 GHz.
+FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
 
 
 BOX = {"large_tilting": "2x1x1 m tilting 0->15 deg/1 s", "dam_break": "1.0x0.6x0.6 m tank, walls on a 2r grid",
@@ -290,7 +297,12 @@ def run_ours(args, world, rank, local, dist):
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic,
                      "ncu_utilisation": measured_limits(args.workload, n, dom),
-                     "stage_ms": stage_ms},
+                     "stage_ms": stage_ms,
+                     "fp32": {"flop_per_particle_step": STEP_FLOP,
+                              "achieved_tflops": STEP_FLOP * value / world / 1e12,   # per GPU
+                              "peak_tflops": FP32_PEAK_TFLOPS, "peak_source": "nominal",
+                              "frac": STEP_FLOP * value / world / 1e12 / FP32_PEAK_TFLOPS,
+                              "dominant_kernel_fma_pipe": (measured_limits(args.workload, n, dom) or {}).get("fma_pipe")}},
     }
     line.update(extras)
     if not args.no_cpu_baseline:

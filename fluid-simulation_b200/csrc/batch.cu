@@ -372,7 +372,7 @@ static void build_batch(BatchSim& B, const wcsph_params& p, const wcsph_batch_sc
     B.scene_first.push_back(B.n);
     WCSPH_CUDA(cudaMemcpyAsync(B.scene_offsets.ptr, B.scene_first.data(), sizeof(u32) * (S + 1ull),
                                cudaMemcpyHostToDevice, B.stream));
-    B.barrier.alloc(2);
+    B.barrier.alloc(8);   // grid-barrier words and the persistent kernel's work counters
     WCSPH_CUDA(cudaMemsetAsync(B.barrier.ptr, 0, B.barrier.bytes(), B.stream));
     B.st.alloc(1);
     B.scenes.alloc(S);

@@ -23,7 +23,7 @@ struct PersistentStep {
     u64* table;
     u32 table_size;
     float cs;
-    u32* barrier;            // [arrivals, generation], both zero between launches
+    u32* barrier;            // [arrivals, generation] (zero between launches), then work counters
     int steps;
     u32 spin_limit;          // look-back polls
     u32 barrier_limit;       // grid-barrier polls (64 ns apart)

@@ -33,12 +33,25 @@ constexpr u32 STOP_FLAGS = ERR_LOOKBACK_TIMEOUT | ERR_BARRIER_TIMEOUT;
 
 __device__ __forceinline__ u32 ld_volatile(const u32* p) { return *reinterpret_cast<const volatile u32*>(p); }
 
+// Work counters of the traversal phases (after the barrier words): warps take
+// CLAIM chunks at a time, so that no block idles at a barrier while others
+// still hold a long queue. Block 0 clears them with the sort plan of each step.
+enum : u32 { WORK_DENSITY = 2, WORK_FORCE = 3, WORK_SURFACE = 4, BARRIER_WORDS = 5 };
+constexpr u32 CLAIM = 4;
+
+__device__ __forceinline__ u32 claim(u32* ctr) {
+    u32 v = 0;
+    if ((threadIdx.x & 31u) == 0) v = atomicAdd(ctr, CLAIM);
+    return __shfl_sync(0xffffffffu, v, 0);
+}
+
 // Grid-wide barrier of the cooperative launch. bar[0] counts arrivals, bar[1]
 // is the generation: the last arriving block resets the count and advances
 // the generation, the others poll it (bounded). Writes of every block before
 // the barrier are visible to every block after it (fences on both sides, as
 // a cooperative-groups grid sync). Returns false once an error stops the step.
 __device__ __forceinline__ bool grid_barrier(u32* bar, DevState* st, u32 limit) {
+    __shared__ u32 s_go;   // the block's decision, the same for all its threads
     __syncthreads();
     if (threadIdx.x == 0) {
         const u32 gen = ld_volatile(bar + 1);
@@ -58,9 +71,10 @@ __device__ __forceinline__ bool grid_barrier(u32* bar, DevState* st, u32 limit) 
             }
         }
         __threadfence();
+        s_go = (ld_volatile(&st->error_flags) & STOP_FLAGS) == 0u ? 1u : 0u;
     }
     __syncthreads();
-    return (ld_volatile(&st->error_flags) & STOP_FLAGS) == 0u;
+    return s_go != 0u;
 }
 
 size_t persistent_smem(const TravArgs& a) {
@@ -88,8 +102,6 @@ __global__ void __launch_bounds__(PTHREADS, 3) persistent_ensemble_kernel(const 
     const u32 tid = threadIdx.x;
     const u32 warp = tid >> 5;
     const u32 nthreads = gridDim.x * PTHREADS;
-    const u32 gwarp = blockIdx.x * PWARPS + warp;
-    const u32 nwarps = gridDim.x * PWARPS;
     const size_t first = static_cast<size_t>(blockIdx.x) * PTHREADS + tid;
     const size_t nlb = static_cast<size_t>(SORT_DIGITS) * ps.tiles * 256u;
     const float np_dt = a.delta < a.np_max_dt ? a.delta : a.np_max_dt;
@@ -102,7 +114,10 @@ __global__ void __launch_bounds__(PTHREADS, 3) persistent_ensemble_kernel(const 
         sortdev::keys_hist_block(ps.pos_state, n, ps.cs, ps.keys[0], ps.hist, ps.scene_state,
                                  reinterpret_cast<u32(*)[256]>(smem), blockIdx.x * PTHREADS, nthreads);
         if (!grid_barrier(ps.barrier, st, ps.barrier_limit)) return;
-        if (blockIdx.x == 0) sortdev::sort_plan_block(n, ps.hist, ps.offsets, st, s_active);
+        if (blockIdx.x == 0) {
+            sortdev::sort_plan_block(n, ps.hist, ps.offsets, st, s_active);
+            if (tid < 3) ps.barrier[WORK_DENSITY + tid] = 0u;
+        }
         if (!grid_barrier(ps.barrier, st, ps.barrier_limit)) return;
         for (int p = 0; p < SORT_DIGITS; ++p) {
             if (!ld_volatile(&st->sort_active[p])) continue;   // the same for every block
@@ -126,30 +141,37 @@ __global__ void __launch_bounds__(PTHREADS, 3) persistent_ensemble_kernel(const 
                                     const_cast<u64*>(a.ckey), ps.table, const_cast<u32*>(a.fluid.cstart),
                                     const_cast<u32*>(a.fluid.cend), a.fluid.tmask, st, ps.scene_state, base + tid);
         if (!grid_barrier(ps.barrier, st, ps.barrier_limit)) return;
+        const u32 nchunks = (n + a.chunk - 1) / a.chunk;
         {
             const WarpView<PASS_DENSITY> S = warp_view<PASS_DENSITY>(a, smem, warp);
-            for (u32 c = gwarp; static_cast<size_t>(c) * a.chunk < n; c += nwarps)
-                cell_pass_chunk<PASS_DENSITY, true>(P, a, S, c, 0.f, 0.f, rm, rs, rs2);
+            for (u32 c0 = claim(ps.barrier + WORK_DENSITY); c0 < nchunks; c0 = claim(ps.barrier + WORK_DENSITY))
+                for (u32 c = c0; c < min(c0 + CLAIM, nchunks); ++c)
+                    cell_pass_chunk<PASS_DENSITY, true>(P, a, S, c, 0.f, 0.f, rm, rs, rs2);
         }
         if (!grid_barrier(ps.barrier, st, ps.barrier_limit)) return;
         const u32 rows = list_rows_per_warp(a.chunk);
+        const u32 ngroups = (n + rows - 1) / rows;
         if (a.nbr) {
-            for (u32 g = gwarp; static_cast<size_t>(g) * rows < n; g += nwarps)
-                list_rows<PASS_FORCE, true>(P, a, g * rows, min(rows, n - g * rows), 0.f, 0.f, rm, rs, rs2);
+            for (u32 g0 = claim(ps.barrier + WORK_FORCE); g0 < ngroups; g0 = claim(ps.barrier + WORK_FORCE))
+                for (u32 g = g0; g < min(g0 + CLAIM, ngroups); ++g)
+                    list_rows<PASS_FORCE, true>(P, a, g * rows, min(rows, n - g * rows), 0.f, 0.f, rm, rs, rs2);
         } else {
             const WarpView<PASS_FORCE> S = warp_view<PASS_FORCE>(a, smem, warp);
-            for (u32 c = gwarp; static_cast<size_t>(c) * a.chunk < n; c += nwarps)
-                cell_pass_chunk<PASS_FORCE, true>(P, a, S, c, 0.f, 0.f, rm, rs, rs2);
+            for (u32 c0 = claim(ps.barrier + WORK_FORCE); c0 < nchunks; c0 = claim(ps.barrier + WORK_FORCE))
+                for (u32 c = c0; c < min(c0 + CLAIM, nchunks); ++c)
+                    cell_pass_chunk<PASS_FORCE, true>(P, a, S, c, 0.f, 0.f, rm, rs, rs2);
         }
         if (!grid_barrier(ps.barrier, st, ps.barrier_limit)) return;
         const float dt = cfl_time_step(a, P);   // fixed step: the bounds alone decide
         if (a.nbr) {
-            for (u32 g = gwarp; static_cast<size_t>(g) * rows < n; g += nwarps)
-                list_rows<PASS_SURFACE, true>(P, a, g * rows, min(rows, n - g * rows), dt, np_dt, rm, rs, rs2);
+            for (u32 g0 = claim(ps.barrier + WORK_SURFACE); g0 < ngroups; g0 = claim(ps.barrier + WORK_SURFACE))
+                for (u32 g = g0; g < min(g0 + CLAIM, ngroups); ++g)
+                    list_rows<PASS_SURFACE, true>(P, a, g * rows, min(rows, n - g * rows), dt, np_dt, rm, rs, rs2);
         } else {
             const WarpView<PASS_SURFACE> S = warp_view<PASS_SURFACE>(a, smem, warp);
-            for (u32 c = gwarp; static_cast<size_t>(c) * a.chunk < n; c += nwarps)
-                cell_pass_chunk<PASS_SURFACE, true>(P, a, S, c, dt, np_dt, rm, rs, rs2);
+            for (u32 c0 = claim(ps.barrier + WORK_SURFACE); c0 < nchunks; c0 = claim(ps.barrier + WORK_SURFACE))
+                for (u32 c = c0; c < min(c0 + CLAIM, nchunks); ++c)
+                    cell_pass_chunk<PASS_SURFACE, true>(P, a, S, c, dt, np_dt, rm, rs, rs2);
         }
         if (!grid_barrier(ps.barrier, st, ps.barrier_limit)) return;
     }

@@ -333,6 +333,20 @@ int wcsph_sample_icosphere(const float center[3], float radius, int level, float
     return WCSPH_OK;
 }
 
+int wcsph_load_obj(const char* path, int normalize, const float model[16], float* vertices_out,
+                   uint32_t* n_triangles) {
+    if (!path || !n_triangles) return WCSPH_ERR_INVALID_ARGUMENT;
+    wcsph_host::Status st;
+    const std::vector<float> t = wcsph_host::load_obj_triangles(path, normalize != 0, model, &st);
+    if (!st.ok()) {
+        g_last_error = st.message;
+        return st.code;
+    }
+    *n_triangles = static_cast<uint32_t>(t.size() / 9);
+    if (vertices_out) std::memcpy(vertices_out, t.data(), sizeof(float) * t.size());
+    return WCSPH_OK;
+}
+
 int wcsph_sample_triangles(const float* vertices, uint32_t n_triangles, float voxel, float* pos_out,
                            uint32_t* n_out) {
     if ((!vertices && n_triangles) || !n_out || !(voxel > 0.f)) return WCSPH_ERR_INVALID_ARGUMENT;

@@ -7,7 +7,20 @@
 
 #include "radix_sort.cuh"
 
+// The persistent ensemble kernel rewrites the sort buffers within one launch
+// and includes this file with WCSPH_COHERENT_LOADS 1: pointer arguments then
+// carry no __restrict__, so that no load takes the non-coherent read-only path.
+#ifndef WCSPH_COHERENT_LOADS
+#define WCSPH_COHERENT_LOADS 0
+#endif
+#if WCSPH_COHERENT_LOADS
+#define WCSPH_SORT_RESTRICT
+#else
+#define WCSPH_SORT_RESTRICT __restrict__
+#endif
+
 namespace wcsph {
+namespace {   // internal linkage: each translation unit has its own flavour
 namespace sortdev {
 
 __device__ __forceinline__ u32 lanemask_lt() {
@@ -41,9 +54,9 @@ __device__ __forceinline__ void flush_hist(u32 (*s_hist)[256], u32* hist) {
 // One block: keys of particles base + threadIdx.x for base = first, first +
 // stride, ... (< n) into keys_out, and their 8 digit histograms added to hist.
 // With `scene` (batched ensembles) the key is batch_key(scene[i], cell).
-__device__ __forceinline__ void keys_hist_block(const float4* __restrict__ pos, u32 n, float cs,
-                                                u64* __restrict__ keys_out, u32* __restrict__ hist,
-                                                const u32* __restrict__ scene, u32 (*s_hist)[256], u32 first,
+__device__ __forceinline__ void keys_hist_block(const float4* WCSPH_SORT_RESTRICT pos, u32 n, float cs,
+                                                u64* WCSPH_SORT_RESTRICT keys_out, u32* WCSPH_SORT_RESTRICT hist,
+                                                const u32* WCSPH_SORT_RESTRICT scene, u32 (*s_hist)[256], u32 first,
                                                 u32 stride) {
     for (int t = threadIdx.x; t < SORT_DIGITS * 256; t += blockDim.x) (&s_hist[0][0])[t] = 0;
     __syncthreads();
@@ -66,8 +79,8 @@ __device__ __forceinline__ void keys_hist_block(const float4* __restrict__ pos, 
 // One block of at least 256 threads: exclusive digit offsets of every pass
 // (and the histograms cleared for the next sort), which passes are trivial,
 // and the ping-pong buffer plan.
-__device__ __forceinline__ void sort_plan_block(u32 n, u32* __restrict__ hist, u32* __restrict__ offsets,
-                                                DevState* __restrict__ st, u32* s_active) {
+__device__ __forceinline__ void sort_plan_block(u32 n, u32* WCSPH_SORT_RESTRICT hist, u32* WCSPH_SORT_RESTRICT offsets,
+                                                DevState* WCSPH_SORT_RESTRICT st, u32* s_active) {
     // one warp per digit pass: lane l scans buckets 8l .. 8l + 7 serially,
     // then the lanes' totals are scanned across the warp (no block barriers)
     const u32 t = threadIdx.x;
@@ -125,10 +138,10 @@ __device__ __forceinline__ void sort_plan_block(u32 n, u32* __restrict__ hist, u
 // (bounded by spin_limit), scatter. Tiles must be claimed in increasing order
 // by running blocks (an atomic counter), so that every tile a look-back waits
 // for is already being processed.
-__device__ __forceinline__ void onesweep_tile(u32 n, int pass, u64* __restrict__ k0, u64* __restrict__ k1,
-                                              u64* __restrict__ k2, u32* __restrict__ v1, u32* __restrict__ v2,
-                                              const u32* __restrict__ offsets, u32* __restrict__ lookback, u32 tiles,
-                                              DevState* __restrict__ st, u32 spin_limit, u32 stall_first_tile,
+__device__ __forceinline__ void onesweep_tile(u32 n, int pass, u64* WCSPH_SORT_RESTRICT k0, u64* WCSPH_SORT_RESTRICT k1,
+                                              u64* WCSPH_SORT_RESTRICT k2, u32* WCSPH_SORT_RESTRICT v1, u32* WCSPH_SORT_RESTRICT v2,
+                                              const u32* WCSPH_SORT_RESTRICT offsets, u32* WCSPH_SORT_RESTRICT lookback, u32 tiles,
+                                              DevState* WCSPH_SORT_RESTRICT st, u32 spin_limit, u32 stall_first_tile,
                                               u32 tile, u32 (*s_wcnt)[256], u32* s_base) {
     constexpr int NW = SORT_THREADS / 32;
     const u32 sel_in = st->sort_sel[pass];
@@ -237,4 +250,5 @@ __device__ __forceinline__ void onesweep_tile(u32 n, int pass, u64* __restrict__
 }
 
 }  // namespace sortdev
+}  // namespace
 }  // namespace wcsph

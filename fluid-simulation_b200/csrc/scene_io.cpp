@@ -8,6 +8,8 @@
 #include <cmath>
 #include <cstring>
 #include <fstream>
+#include <limits>
+#include <sstream>
 #include <vector>
 
 namespace wcsph_host {
@@ -292,6 +294,90 @@ std::vector<float> icosphere_triangles(const float center[3], float radius, int 
     for (const auto& tr : f)
         for (int k = 0; k < 3; ++k)
             for (int d = 0; d < 3; ++d) out.push_back(static_cast<float>(center[d] + radius * v[tr[k]][d]));
+    return out;
+}
+
+// ----------------------------------------------------------- .obj meshes --
+// Geometry::from_file (src/render/geometry.cpp:50-140, tinyobjloader) and
+// Geometry::load_triangles (geometry.cpp:185-207): vertex positions of the
+// first shape's faces in file order, faces of more than three vertices
+// rejected with the reference's message, optional normalisation into a unit
+// box around the origin (with the reference's starting maximum of
+// numeric_limits<float>::min()), then model * (x, y, z, 1). A new shape
+// starts at an `o` or `g` line that follows faces; later shapes are ignored.
+// Face vertices may be written v, v/vt, v//vn or v/vt/vn, with negative
+// indices counting back from the last vertex.
+std::vector<float> load_obj_triangles(const std::string& path, bool normalize, const float* model, Status* status) {
+    auto fail = [&](int code, const std::string& msg) {
+        if (status) *status = Status{code, msg};
+        return std::vector<float>{};
+    };
+    std::ifstream in(path);
+    if (!in) return fail(WCSPH_ERR_IO, "failed to load " + path);
+    std::vector<float> v;    // x, y, z per vertex
+    std::vector<float> out;  // 9 floats per triangle
+    std::string line;
+    bool faces_seen = false;
+    size_t face = 0;
+    while (std::getline(in, line)) {
+        std::istringstream ls(line);
+        std::string tag;
+        if (!(ls >> tag)) continue;
+        if (tag == "v") {
+            float x = 0.f, y = 0.f, z = 0.f;
+            if (!(ls >> x >> y >> z)) return fail(WCSPH_ERR_IO, "failed to load " + path + ": bad vertex line");
+            v.insert(v.end(), {x, y, z});
+        } else if (tag == "o" || tag == "g") {
+            if (faces_seen) break;   // the first shape ends here
+        } else if (tag == "f") {
+            std::vector<long> idx;
+            std::string tok;
+            while (ls >> tok) {
+                const long k = std::strtol(tok.c_str(), nullptr, 10);   // vertex index before any '/'
+                const long nv = static_cast<long>(v.size() / 3);
+                const long i = k > 0 ? k - 1 : nv + k;
+                if (k == 0 || i < 0 || i >= nv)
+                    return fail(WCSPH_ERR_IO, "failed to load " + path + ": face " + std::to_string(face) +
+                                                  " refers to a missing vertex");
+                idx.push_back(i);
+            }
+            if (idx.size() > 3)
+                return fail(WCSPH_ERR_INVALID_ARGUMENT, "In " + path + ": face " + std::to_string(face) + " has " +
+                                                            std::to_string(idx.size()) + " vertices (not a triangle)");
+            if (idx.size() == 3)
+                for (long i : idx) out.insert(out.end(), {v[3 * i], v[3 * i + 1], v[3 * i + 2]});
+            faces_seen = true;
+            ++face;
+        }
+    }
+    if (normalize && !out.empty()) {
+        float mn[3], mx[3];
+        for (int d = 0; d < 3; ++d) {
+            mn[d] = std::numeric_limits<float>::max();
+            mx[d] = std::numeric_limits<float>::min();
+        }
+        for (size_t k = 0; k < out.size(); k += 3)
+            for (int d = 0; d < 3; ++d) {
+                mn[d] = std::min(mn[d], out[k + d]);
+                mx[d] = std::max(mx[d], out[k + d]);
+            }
+        float c[3], diff[3];
+        for (int d = 0; d < 3; ++d) {
+            c[d] = (mn[d] + mx[d]) * 0.5f;
+            diff[d] = mx[d] - mn[d];
+        }
+        const float md = std::max(std::max(diff[0], diff[1]), diff[2]);
+        for (size_t k = 0; k < out.size(); k += 3)
+            for (int d = 0; d < 3; ++d) out[k + d] = (out[k + d] - c[d]) / md;
+    }
+    if (model) {
+        for (size_t k = 0; k < out.size(); k += 3) {
+            const float x = out[k], y = out[k + 1], z = out[k + 2];
+            for (int d = 0; d < 3; ++d)
+                out[k + d] = model[d] * x + model[4 + d] * y + model[8 + d] * z + model[12 + d];
+        }
+    }
+    if (status) *status = Status{};
     return out;
 }
 

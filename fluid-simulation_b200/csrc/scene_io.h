@@ -30,5 +30,9 @@ void make_velocities(uint32_t n, float sigma, uint64_t seed, float* out);
 uint32_t sample_box_walls(const float mn[3], const float mx[3], float spacing, float* out);
 uint32_t sample_triangles(const float* verts, uint32_t ntri, float voxel, float* out);
 std::vector<float> icosphere_triangles(const float center[3], float radius, int level);
+// Triangles (9 floats each) of the first shape of a Wavefront .obj file,
+// optionally normalised, then transformed by a column-major model matrix
+// (NULL = identity). Fills *status on failure and returns no triangles.
+std::vector<float> load_obj_triangles(const std::string& path, bool normalize, const float* model, Status* status);
 
 }  // namespace wcsph_host

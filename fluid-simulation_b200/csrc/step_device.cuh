@@ -7,7 +7,9 @@
 // (ld.global.nc) in the per-pass kernels. The persistent kernel rewrites the
 // same buffers within one launch (hash, sorted state, records, lists, every
 // step), for which the read-only path is not coherent; it includes this file
-// with WCSPH_COHERENT_LOADS 1, which makes those loads ordinary global loads.
+// with WCSPH_COHERENT_LOADS 1, which makes those loads ordinary global loads
+// and drops the __restrict__ of pointer arguments (through which the compiler
+// may otherwise choose the read-only path by itself).
 // Everything here has internal linkage, so both variants can coexist.
 #pragma once
 #include <climits>
@@ -19,8 +21,10 @@
 #endif
 #if WCSPH_COHERENT_LOADS
 #define WCSPH_RO_QUAL ""
+#define WCSPH_RESTRICT
 #else
 #define WCSPH_RO_QUAL ".nc"
+#define WCSPH_RESTRICT __restrict__
 #endif
 
 namespace wcsph {
@@ -38,7 +42,7 @@ __device__ __forceinline__ T ro_ld(const T* p) {
 // Linear-probed lookup of a packed cell key (find_cell_in_table,
 // common.cuh:89-102), with the loads of this file's flavour.
 template <bool BATCH = false>
-__device__ __forceinline__ u32 find_slot(const u64* __restrict__ table, u32 tmask, u64 pk) {
+__device__ __forceinline__ u32 find_slot(const u64* WCSPH_RESTRICT table, u32 tmask, u64 pk) {
     u32 t = static_cast<u32>(slot_hash<BATCH>(pk) & tmask);
     for (u32 j = 0; j <= tmask; ++j) {
         const u64 k = ro_ld(table + t);
@@ -103,7 +107,7 @@ struct KindCfg {
     // resident warps per SM the register allocation must allow (32 -> 64 registers,
     // 28 -> 72, 24 -> 80, 16 -> 128): the density pass spills a little at 72
     // registers, which costs less than fewer resident warps at 80; the force
-    // pass below 80, the adjoint force pass below 128
+    // pass spills below 80 and the adjoint force pass below 128
     static constexpr int min_warps = KIND == PASS_DENSITY ? 28
                                      : KIND == PASS_SURFACE ? 32 : (KIND == PASS_ADJ_FORCE ? 16 : 24);
 };
@@ -652,7 +656,7 @@ __device__ __forceinline__ float4 home_x(const WarpView<PASS_DENSITY>& S, const 
 // i0 + k, nbr[r * n + i0 + k], for r < nbr_width.
 template <int KIND, bool SHARED_BITS = false>
 __device__ __forceinline__ u32 fluid_hit_run(const WarpView<KIND>& S, const DevParams& P, const TravArgs& a,
-                                             const u32* __restrict__ bits, u32 nh, u32 M, u32 i0, u32& lo,
+                                             const u32* WCSPH_RESTRICT bits, u32 nh, u32 M, u32 i0, u32& lo,
                                              u32& hi, bool lists = false, HomeMap hm = HomeMap{32u, NO_HOME, 0u}) {
     auto home = [&](u32 k) -> HomeData {
         if constexpr (KIND == PASS_DENSITY) {
@@ -761,13 +765,31 @@ __device__ __forceinline__ u32 fluid_hit_run(const WarpView<KIND>& S, const DevP
 __device__ __forceinline__ void density_test_words(const WarpView<PASS_DENSITY>& S, const DevParams& P,
                                                    const TravArgs& a, u32 nh, u32 wpr, u32 i0, HomeMap hm,
                                                    u32 win_a, u32 win_b) {
-    const u32 nwords = nh * wpr;
     const float2 neg = make_float2(-1.f, -1.f);
-    // w / wpr as a multiply-high: exact for w < 2^32 / wpr^2 (here w < 32 * 16)
-    const u32 inv = 0xFFFFFFFFu / wpr + 1u;
-    for (u32 w = lane_id(); w < nwords; w += 32) {
-        const u32 k = wpr == 1u ? w : __umulhi(w, inv);
-        const u32 wi = w - k * wpr;
+    // rows [0, na) test words [0, wa) only, rows [na, nh) words [wb0, wpr) only:
+    // the words that hold their window; the others of the row read zero
+    const u32 na = min(hm.split, nh), nb = nh - na;
+    const u32 wa = min(wpr, (win_a + 31u) >> 5);
+    const u32 wb0 = min(wpr, win_b >> 5), wb = wpr - wb0;
+    const u32 ta = na * wa, total = ta + nb * wb;
+    if (total < nh * wpr) {
+        for (u32 w = lane_id(); w < nh * wpr; w += 32) S.aux[w] = 0u;
+        __syncwarp();
+    }
+    // w / wa, w / wb as multiply-highs: exact for w < 2^32 / d^2 (here w < 32 * 16)
+    const u32 inv_a = 0xFFFFFFFFu / max(wa, 1u) + 1u;
+    const u32 inv_b = 0xFFFFFFFFu / max(wb, 1u) + 1u;
+    for (u32 w = lane_id(); w < total; w += 32) {
+        u32 k, wi;
+        if (w < ta) {
+            k = wa == 1u ? w : __umulhi(w, inv_a);
+            wi = w - k * wa;
+        } else {
+            const u32 w2 = w - ta;
+            const u32 kb = wb == 1u ? w2 : __umulhi(w2, inv_b);
+            k = na + kb;
+            wi = wb0 + (w2 - kb * wb);
+        }
         const float4 h = home_x(S, a, i0, hm, k);
         const float2 X = make_float2(h.x, h.x), Y = make_float2(h.y, h.y), Z = make_float2(h.z, h.z);
         const float2* base = S.sp + pair_slot(wi * 16u);
@@ -781,11 +803,11 @@ __device__ __forceinline__ void density_test_words(const WarpView<PASS_DENSITY>&
             bits |= (r2.x <= P.h2 ? 1u << (2 * t) : 0u) | (r2.y <= P.h2 ? 2u << (2 * t) : 0u);
         }
         // candidates [lo, hi) of the row's window within this word
-        const u32 lo = k < hm.split ? 0u : win_b, hi = k < hm.split ? win_a : 0xFFFFFFFFu;
+        const u32 lo = k < na ? 0u : win_b, hi = k < na ? win_a : 0xFFFFFFFFu;
         const u32 w0 = wi << 5;
         if (lo > w0) bits &= lo >= w0 + 32u ? 0u : FULL << (lo - w0);
         if (hi < w0 + 32u) bits &= hi <= w0 ? 0u : FULL >> (w0 + 32u - hi);
-        S.aux[w] = bits;
+        S.aux[k * wpr + wi] = bits;
     }
     __syncwarp();
 }
@@ -1451,12 +1473,12 @@ __device__ __forceinline__ u64 cell_key_of(float4 p, float cs, const u32* scene_
 // cell keys, run starts/ends into the hash; rebuild_n_search.cu:19-34). All 32
 // lanes of a warp must call it together (i >= n for the idle ones).
 template <bool BATCH>
-__device__ __forceinline__ void reorder_cell_item(const float4* __restrict__ pos_in, const float4* __restrict__ vel_in,
-                                                  const u32* __restrict__ v1, const u32* __restrict__ v2,
-                                                  const DevState* st, u32 n, float cs, float4* __restrict__ pos_out,
-                                                  float4* __restrict__ vel_out, u32* __restrict__ perm_out,
-                                                  u64* __restrict__ ckey_out, u64* table, u32* cstart, u32* cend,
-                                                  u32 tmask, DevState* st_err, const u32* __restrict__ scene_in, u32 i) {
+__device__ __forceinline__ void reorder_cell_item(const float4* WCSPH_RESTRICT pos_in, const float4* WCSPH_RESTRICT vel_in,
+                                                  const u32* WCSPH_RESTRICT v1, const u32* WCSPH_RESTRICT v2,
+                                                  const DevState* st, u32 n, float cs, float4* WCSPH_RESTRICT pos_out,
+                                                  float4* WCSPH_RESTRICT vel_out, u32* WCSPH_RESTRICT perm_out,
+                                                  u64* WCSPH_RESTRICT ckey_out, u64* table, u32* cstart, u32* cend,
+                                                  u32 tmask, DevState* st_err, const u32* WCSPH_RESTRICT scene_in, u32 i) {
     const u32 lane = threadIdx.x & 31u;
     const u32 sel = st->sort_sel[8];
     const u32* perm = sel == 0 ? nullptr : (sel == 1 ? v1 : v2);

@@ -181,6 +181,7 @@ def load_library(path: str | os.PathLike | None = None) -> C.CDLL:
         "wcsph_sample_box_walls": (C.c_int, [f, f, C.c_float, f, C.POINTER(C.c_uint32)]),
         "wcsph_sample_icosphere": (C.c_int, [f, C.c_float, C.c_int, C.c_float, f, C.POINTER(C.c_uint32)]),
         "wcsph_sample_triangles": (C.c_int, [f, C.c_uint32, C.c_float, f, C.POINTER(C.c_uint32)]),
+        "wcsph_load_obj": (C.c_int, [C.c_char_p, C.c_int, f, f, C.POINTER(C.c_uint32)]),
         "wcsph_preset": (C.c_int, [C.c_char_p, C.c_uint64, C.POINTER(PresetInfo), f, f, f]),
         "wcsph_preset_box": (C.c_int, [C.c_char_p, C.c_int64, C.c_float, C.POINTER(Box)]),
         "wcsph_preset_ensemble": (C.c_int, [C.c_uint64, C.c_uint32, C.POINTER(PresetInfo), f, f, f]),
@@ -290,6 +291,29 @@ def sample_icosphere(center, radius, level, voxel) -> np.ndarray:
     out = np.empty((cnt.value, 4), np.float32)
     _check(lib.wcsph_sample_icosphere((C.c_float * 3)(*center), radius, level, voxel, fptr(out),
                                       C.byref(cnt)), None)
+    return out
+
+
+def load_obj(path, normalize: bool = False, model: np.ndarray | None = None) -> np.ndarray:
+    """Triangles [n, 3, 3] of the first shape of a .obj mesh (wcsph_load_obj:
+    the reference's Geometry::from_file + load_triangles)."""
+    lib = load_library()
+    m = None if model is None else np.ascontiguousarray(model, np.float32).reshape(16)
+    n = C.c_uint32()
+    _check(lib.wcsph_load_obj(str(path).encode(), int(normalize), fptr(m), None, C.byref(n)), None)
+    out = np.empty((n.value, 3, 3), np.float32)
+    _check(lib.wcsph_load_obj(str(path).encode(), int(normalize), fptr(m), fptr(out), C.byref(n)), None)
+    return out
+
+
+def sample_triangles(tris: np.ndarray, voxel: float) -> np.ndarray:
+    """Boundary particles of a triangle soup by surface voxelisation (wcsph_sample_triangles)."""
+    lib = load_library()
+    t = np.ascontiguousarray(tris, np.float32).reshape(-1, 9)
+    n = C.c_uint32()
+    _check(lib.wcsph_sample_triangles(fptr(t), t.shape[0], voxel, None, C.byref(n)), None)
+    out = np.empty((n.value, 4), np.float32)
+    _check(lib.wcsph_sample_triangles(fptr(t), t.shape[0], voxel, fptr(out), C.byref(n)), None)
     return out
 
 

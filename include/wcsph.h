@@ -263,6 +263,15 @@ int wcsph_sample_icosphere(const float center[3], float radius, int level, float
 /* Surface voxelisation of an arbitrary triangle soup (float3 per vertex).   */
 int wcsph_sample_triangles(const float* vertices, uint32_t n_triangles, float voxel,
                            float* pos_out, uint32_t* n_out);
+/* Triangles of a Wavefront .obj mesh, for wcsph_sample_triangles: replaces
+ * Geometry::from_file + Geometry::load_triangles (src/render/geometry.cpp:50-140,
+ * 185-207; tinyobjloader). The first shape's faces in file order; a face of
+ * more than three vertices is rejected as there (WCSPH_ERR_INVALID_ARGUMENT,
+ * "In <path>: face f has N vertices (not a triangle)"); normalize != 0 scales
+ * the mesh into a unit box around the origin; model (column-major 4x4, NULL =
+ * identity) is applied last. Call with vertices_out = NULL for the count.   */
+int wcsph_load_obj(const char* path, int normalize, const float model[16], float* vertices_out,
+                   uint32_t* n_triangles);
 
 /* ---- workload presets -------------------------------------------------------
  * Scenes of the reference's headless apps that need no missing asset

@@ -52,9 +52,10 @@ def one(name: str, out_dir: Path):
     print(name, "ok", int(cnt.sum()), "neighbour pairs", flush=True)
 
 
-def trajectory(name: str, out_dir: Path, steps: int, full: set[int], skip: int = 0):
+def trajectory(name: str, out_dir: Path, steps: int, full: set[int], skip: int = 0, vy: float = 0.0):
     """The reference's own trajectory of `steps` steps, after `skip` unrecorded
-    steps from the scene's initial state, one directory per recorded step: the
+    steps from the scene's initial state (with `vy` added to every fluid
+    particle's initial y velocity), one directory per recorded step: the
     step's input state (in_pos, in_vel),
     its sorted keys, permutation, (dt, np_dt), density, pressure and neighbour
     counts; steps in `full` also keep every field and the neighbour lists.
@@ -63,6 +64,9 @@ def trajectory(name: str, out_dir: Path, steps: int, full: set[int], skip: int =
     import refpath
 
     p, bx, pos, vel, bpos, delta = scene_of(name)
+    if vy:
+        vel = np.array(vel, np.float32, copy=True)
+        vel[:, 1] += np.float32(vy)
     box_at = None
     if name not in __import__("fixtures").NAMES:
         import wcsph
@@ -116,14 +120,15 @@ def trajectory(name: str, out_dir: Path, steps: int, full: set[int], skip: int =
 
 
 def main():
-    # make_ref_fixtures.py [out_dir [scene [--trajectory STEPS [--skip N] [FULL_STEP ...]]]]
+    # make_ref_fixtures.py [out_dir [scene [--trajectory STEPS [--skip N] [--vy V] [FULL_STEP ...]]]]
     out = Path(sys.argv[1]) if len(sys.argv) > 1 else HERE
     if len(sys.argv) > 3 and sys.argv[3] == "--trajectory":
         rest = sys.argv[5:]
-        skip = 0
-        if rest[:1] == ["--skip"]:
-            skip, rest = int(rest[1]), rest[2:]
-        trajectory(sys.argv[2], out, int(sys.argv[4]), {int(x) for x in rest}, skip)
+        opt = {"--skip": 0, "--vy": 0.0}
+        while rest[:1] and rest[0] in opt:
+            opt[rest[0]] = type(opt[rest[0]])(rest[1])
+            rest = rest[2:]
+        trajectory(sys.argv[2], out, int(sys.argv[4]), {int(x) for x in rest}, opt["--skip"], opt["--vy"])
         return
     if len(sys.argv) > 2:
         one(sys.argv[2], out)

@@ -82,27 +82,30 @@ def test_cuda_path_matches_reference_kernels(name, tmp_path):
     assert not fails, fails
 
 
-def reference_trajectory(name, steps, full, skip, tmp_path):
+def reference_trajectory(name, steps, full, skip, vy, tmp_path):
     if not refpath.available(name):
         pytest.skip(f"no reference harness for {name}")
     out = tmp_path / f"traj_{name}"
     subprocess.run([sys.executable, str(GEN), str(out), name, "--trajectory", str(steps), "--skip", str(skip),
-                    *map(str, full)], check=True, timeout=1800)
+                    "--vy", str(vy), *map(str, full)], check=True, timeout=1800)
     return out
 
 
-@pytest.mark.parametrize("name,steps,skip,full", [("mesh_obstacle", 50, 450, (0, 1, 25, 49)),
-                                                  ("large_tilting", 10, 0, (0, 9))])
-def test_reference_trajectory_replayed_step_by_step(name, steps, skip, full, tmp_path):
-    """Config 1 (mesh obstacle, CFL 0.4, dt cap 1e-3) for 50 steps from
-    t = 0.45 s, when the collapsing column hits the floor and the sphere at
-    about 4.4 m/s and the CFL rule sets dt, and the 1,048,576-particle tilting
-    box for its first 10 steps of its box schedule: at every
+@pytest.mark.parametrize("name,steps,skip,vy,full", [("mesh_obstacle", 50, 0, 0.0, (0, 1, 25, 49)),
+                                                     ("mesh_obstacle", 50, 0, -8.0, (0, 24, 49)),
+                                                     ("large_tilting", 10, 0, 0.0, (0, 9))])
+def test_reference_trajectory_replayed_step_by_step(name, steps, skip, vy, full, tmp_path):
+    """Config 1 (mesh obstacle, CFL 0.4, dt cap 1e-3) for its first 50 steps,
+    in which the collapsing column stays below the 4 m/s at which the CFL
+    step 0.4 * 2r / max|v| drops under the cap; the same scene thrown down at
+    8 m/s onto the sphere, in which the CFL rule sets dt; and
+    the 1,048,576-particle tilting box for the first 10 steps of its box
+    schedule: at every
     step the CFL step (dt_p, np_dt), sorted Morton keys, permutation and
     neighbour counts equal the reference's and density is within 1e-5; at
     the `full` steps the neighbour lists are compared in reference order and
     every field is checked."""
-    traj = reference_trajectory(name, steps, full, skip, tmp_path)
+    traj = reference_trajectory(name, steps, full, skip, vy, tmp_path)
     pre = wcsph.preset(name)
     p, delta = pre.params, pre.info.delta
     sim = wcsph.CUDASPHSimulator(p, pre.pos, pre.box, fluid_vel=pre.vel, boundary_pos=pre.bpos)
@@ -144,8 +147,7 @@ def test_reference_trajectory_replayed_step_by_step(name, steps, skip, full, tmp
                 assert not fails, f"step {k}: {fails}"
     finally:
         sim.close()
-    if name == "mesh_obstacle":
-        # the replayed steps must exercise the CFL rule, not only the dt cap
-        capped = sum(d == float(np.float32(p.max_time_step)) for d in dts)
-        print(f"{name}: dt from {min(dts):.3g} to {max(dts):.3g}, {steps - capped} of {steps} steps set by CFL")
-        assert capped < steps, dts
+    capped = sum(d == float(np.float32(p.max_time_step)) for d in dts)
+    print(f"{name} (vy {vy}): dt from {min(dts):.4g} to {max(dts):.4g}, {steps - capped} of {steps} steps set by CFL")
+    if vy:
+        assert capped <= steps // 2, dts   # the thrown scene runs mostly on the CFL step
