@@ -79,6 +79,16 @@ __host__ __device__ __forceinline__ float4 mat_mul(const float4 m[4], float4 v) 
                        m[0].z * v.x + m[1].z * v.y + m[2].z * v.z + m[3].z * v.w,
                        m[0].w * v.x + m[1].w * v.y + m[2].w * v.z + m[3].w * v.w);
 }
+#ifdef __CUDACC__
+// mat_mul with its rounding written out (the collision response of the step).
+__device__ __forceinline__ float4 mat_mul_rn(const float4 m[4], float4 v) {
+    auto row = [&](float a, float b, float c, float d) {
+        return __fmaf_rn(d, v.w, __fmaf_rn(c, v.z, __fmaf_rn(b, v.y, __fmul_rn(a, v.x))));
+    };
+    return make_float4(row(m[0].x, m[1].x, m[2].x, m[3].x), row(m[0].y, m[1].y, m[2].y, m[3].y),
+                       row(m[0].z, m[1].z, m[2].z, m[3].z), row(m[0].w, m[1].w, m[2].w, m[3].w));
+}
+#endif
 
 // Squared distance used by the neighbour predicate (is_neighbor,
 // common.cuh:39-47, with dot() of math.cuh:54-56). The reference's

@@ -342,8 +342,8 @@ __device__ __forceinline__ float4 f4(float x, float y, float z, float w = 0.f) {
 
 // Box collision (resolve_collisions, update_positions.cu:14-52).
 __device__ __forceinline__ void resolve_collision(float4& x, float4& v, const DevBox& bb, const DevParams& P) {
-    float4 pos = mat_mul(bb.model_inv, x);
-    float4 vel = mat_mul(bb.model_inv, v);
+    float4 pos = mat_mul_rn(bb.model_inv, x);
+    float4 vel = mat_mul_rn(bb.model_inv, v);
     bool changed = false;
     const float buf = P.collision_buffer;
     if (pos.x - buf < bb.min.x) { pos.x = bb.min.x + P.radius; vel.x *= -P.elasticity; changed = true; }
@@ -353,8 +353,8 @@ __device__ __forceinline__ void resolve_collision(float4& x, float4& v, const De
     if (pos.z - buf < bb.min.z) { pos.z = bb.min.z + P.radius; vel.z *= -P.elasticity; changed = true; }
     else if (pos.z + buf > bb.max.z) { pos.z = bb.max.z - P.radius; vel.z *= -P.elasticity; changed = true; }
     if (changed) {
-        x = mat_mul(bb.model, pos);
-        v = mat_mul(bb.model, vel);
+        x = mat_mul_rn(bb.model, pos);
+        v = mat_mul_rn(bb.model, vel);
     }
 }
 
@@ -765,31 +765,13 @@ __device__ __forceinline__ u32 fluid_hit_run(const WarpView<KIND>& S, const DevP
 __device__ __forceinline__ void density_test_words(const WarpView<PASS_DENSITY>& S, const DevParams& P,
                                                    const TravArgs& a, u32 nh, u32 wpr, u32 i0, HomeMap hm,
                                                    u32 win_a, u32 win_b) {
+    const u32 nwords = nh * wpr;
     const float2 neg = make_float2(-1.f, -1.f);
-    // rows [0, na) test words [0, wa) only, rows [na, nh) words [wb0, wpr) only:
-    // the words that hold their window; the others of the row read zero
-    const u32 na = min(hm.split, nh), nb = nh - na;
-    const u32 wa = min(wpr, (win_a + 31u) >> 5);
-    const u32 wb0 = min(wpr, win_b >> 5), wb = wpr - wb0;
-    const u32 ta = na * wa, total = ta + nb * wb;
-    if (total < nh * wpr) {
-        for (u32 w = lane_id(); w < nh * wpr; w += 32) S.aux[w] = 0u;
-        __syncwarp();
-    }
-    // w / wa, w / wb as multiply-highs: exact for w < 2^32 / d^2 (here w < 32 * 16)
-    const u32 inv_a = 0xFFFFFFFFu / max(wa, 1u) + 1u;
-    const u32 inv_b = 0xFFFFFFFFu / max(wb, 1u) + 1u;
-    for (u32 w = lane_id(); w < total; w += 32) {
-        u32 k, wi;
-        if (w < ta) {
-            k = wa == 1u ? w : __umulhi(w, inv_a);
-            wi = w - k * wa;
-        } else {
-            const u32 w2 = w - ta;
-            const u32 kb = wb == 1u ? w2 : __umulhi(w2, inv_b);
-            k = na + kb;
-            wi = wb0 + (w2 - kb * wb);
-        }
+    // w / wpr as a multiply-high: exact for w < 2^32 / wpr^2 (here w < 32 * 16)
+    const u32 inv = 0xFFFFFFFFu / wpr + 1u;
+    for (u32 w = lane_id(); w < nwords; w += 32) {
+        const u32 k = wpr == 1u ? w : __umulhi(w, inv);
+        const u32 wi = w - k * wpr;
         const float4 h = home_x(S, a, i0, hm, k);
         const float2 X = make_float2(h.x, h.x), Y = make_float2(h.y, h.y), Z = make_float2(h.z, h.z);
         const float2* base = S.sp + pair_slot(wi * 16u);
@@ -803,11 +785,11 @@ __device__ __forceinline__ void density_test_words(const WarpView<PASS_DENSITY>&
             bits |= (r2.x <= P.h2 ? 1u << (2 * t) : 0u) | (r2.y <= P.h2 ? 2u << (2 * t) : 0u);
         }
         // candidates [lo, hi) of the row's window within this word
-        const u32 lo = k < na ? 0u : win_b, hi = k < na ? win_a : 0xFFFFFFFFu;
+        const u32 lo = k < hm.split ? 0u : win_b, hi = k < hm.split ? win_a : 0xFFFFFFFFu;
         const u32 w0 = wi << 5;
         if (lo > w0) bits &= lo >= w0 + 32u ? 0u : FULL << (lo - w0);
         if (hi < w0 + 32u) bits &= hi <= w0 ? 0u : FULL >> (w0 + 32u - hi);
-        S.aux[k * wpr + wi] = bits;
+        S.aux[w] = bits;
     }
     __syncwarp();
 }
@@ -852,14 +834,18 @@ __device__ __forceinline__ u32 boundary_pair_run(const WarpView<KIND>& S, const 
 
 // Per-row epilogue of a pass: the sums res (fluid) and resb (boundary) of
 // particle i become its fields; the surface pass integrates and adds to
-// the warp's CFL / metric reductions.
+// the warp's CFL / metric reductions. The rounding of every step is written
+// out (__fmaf_rn, __fmul_rn, __fadd_rn): the compiler would otherwise choose
+// which products to fuse by the surrounding code, and the per-pass kernels and
+// the persistent ensemble kernel, which inline this into different code, must
+// produce the same bits.
 template <int KIND, bool BATCH>
 __device__ __forceinline__ void finish_row(const DevParams& P, const TravArgs& a, u32 i, const float* res,
                                            const float* resb, u32 row_cnt, u32 scene, float dt, float np_dt,
                                            float& red_max, float& red_speed, float& red_speed2) {
     if constexpr (KIND == PASS_DENSITY) {
         // compute_density: (W(0) + sum W) * m, then + sum m_b W
-        const float rho = (P.w0 + P.cubic_factor * res[0]) * P.mass + P.cubic_factor * resb[0];
+        const float rho = __fmaf_rn(__fmaf_rn(P.cubic_factor, res[0], P.w0), P.mass, __fmul_rn(P.cubic_factor, resb[0]));
         const float prs = tait_pressure(rho, P);
         a.rho[i] = rho;
         a.prs[i] = prs;
@@ -867,15 +853,15 @@ __device__ __forceinline__ void finish_row(const DevParams& P, const TravArgs& a
         // the force pass's neighbour records
         const float4 xi = a.pos[i];
         const float4 vi = a.vel[i];
-        a.recf[2 * static_cast<size_t>(i)] = make_float4(xi.x, xi.y, xi.z, prs / (rho * rho));
-        a.recf[2 * static_cast<size_t>(i) + 1] = make_float4(vi.x, vi.y, vi.z, 1.f / rho);
+        a.recf[2 * static_cast<size_t>(i)] = make_float4(xi.x, xi.y, xi.z, __fdiv_rn(prs, __fmul_rn(rho, rho)));
+        a.recf[2 * static_cast<size_t>(i) + 1] = make_float4(vi.x, vi.y, vi.z, __fdiv_rn(1.f, rho));
     } else if constexpr (KIND == PASS_FORCE) {
         // compute_pressure_accel_n_normal_with_boundary: m * sum_fluid, then
         // the boundary term (compute_pressure_accel_n_normal.cu:346-364)
-        a.ap[i] = f4(P.mass * res[0] + resb[0], P.mass * res[1] + resb[1],
-                     P.mass * res[2] + resb[2]);
-        const float sn = P.h * P.mass;
-        const float4 ni = f4(sn * res[3], sn * res[4], sn * res[5]);
+        a.ap[i] = f4(__fmaf_rn(P.mass, res[0], resb[0]), __fmaf_rn(P.mass, res[1], resb[1]),
+                     __fmaf_rn(P.mass, res[2], resb[2]));
+        const float sn = __fmul_rn(P.h, P.mass);
+        const float4 ni = f4(__fmul_rn(sn, res[3]), __fmul_rn(sn, res[4]), __fmul_rn(sn, res[5]));
         a.normal[i] = ni;
         a.vlap[i] = f4(res[6], res[7], res[8]);
         // the surface pass's neighbour record
@@ -896,21 +882,24 @@ __device__ __forceinline__ void finish_row(const DevParams& P, const TravArgs& a
             bb = &a.scenes[scene].box;
             a.scene_state[i] = scene;
         }
+        auto accel = [&](float g, float f, float vl, float st) {
+            return __fmaf_rn(-P.st_scale, st, __fmaf_rn(gv.w, vl, __fadd_rn(g, f)));
+        };
         float4 anp;
-        anp.x = gv.x + fe.x + gv.w * vli.x - P.st_scale * res[0];
-        anp.y = gv.y + fe.y + gv.w * vli.y - P.st_scale * res[1];
-        anp.z = gv.z + fe.z + gv.w * vli.z - P.st_scale * res[2];
+        anp.x = accel(gv.x, fe.x, vli.x, res[0]);
+        anp.y = accel(gv.y, fe.y, vli.y, res[1]);
+        anp.z = accel(gv.z, fe.z, vli.z, res[2]);
         anp.w = 0.f;
         a.anp[i] = anp;
-        // update_positions.cu:64-67
+        // update_positions.cu:64-67: v += np_dt a_np + dt a_p; x += dt v
         float4 v = vi, x = xi;
-        v.x += np_dt * anp.x + dt * api.x;
-        v.y += np_dt * anp.y + dt * api.y;
-        v.z += np_dt * anp.z + dt * api.z;
-        x.x += dt * v.x;
-        x.y += dt * v.y;
-        x.z += dt * v.z;
-        x.w += dt * v.w;
+        v.x = __fadd_rn(v.x, __fmaf_rn(np_dt, anp.x, __fmul_rn(dt, api.x)));
+        v.y = __fadd_rn(v.y, __fmaf_rn(np_dt, anp.y, __fmul_rn(dt, api.y)));
+        v.z = __fadd_rn(v.z, __fmaf_rn(np_dt, anp.z, __fmul_rn(dt, api.z)));
+        x.x = __fmaf_rn(dt, v.x, x.x);
+        x.y = __fmaf_rn(dt, v.y, x.y);
+        x.z = __fmaf_rn(dt, v.z, x.z);
+        x.w = __fmaf_rn(dt, v.w, x.w);
         resolve_collision(x, v, *bb, P);
         a.pos_out[i] = x;
         a.vel_out[i] = v;
