@@ -233,6 +233,7 @@ struct BatchSim {
     // k steps in one cooperative launch (graph replay when captured)
     void persistent_steps(int k, float delta) {
         if (k <= 0) return;
+        NvtxRange r("wcsph ensemble: persistent launch");
         prepare_persistent(k, delta);
         if (pgraph && pgraph_delta == delta && pgraph_steps == k) WCSPH_CUDA(cudaGraphLaunch(pgraph, stream));
         else launch_persistent(persistent_args(delta, k), p_blocks, p_smem, stream);

@@ -9,9 +9,14 @@
 #include <cmath>
 #include <cstring>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "tuner.cuh"
 
 namespace wcsph {
+
+NvtxRange::NvtxRange(const char* name) { nvtxRangePushA(name); }
+NvtxRange::~NvtxRange() { nvtxRangePop(); }
 
 void cuda_check(cudaError_t e, const char* what) {
     if (e != cudaSuccess) {
@@ -314,6 +319,7 @@ TravArgs CUDASPHSimulator::trav_args(float delta) {
 }
 
 void CUDASPHSimulator::enqueue_search(bool keys_from_state) {
+    NvtxRange r("wcsph sort + neighbourhood search");
     const u32 n = n_;
     WCSPH_CUDA(cudaMemsetAsync(table_.ptr, 0xff, table_.bytes(), stream_));
     if (keys_from_state) enqueue_keys();
@@ -354,11 +360,21 @@ void CUDASPHSimulator::enqueue_fixed_step(float dt) {
 }
 
 void CUDASPHSimulator::enqueue_step(float delta) {
+    NvtxRange r("wcsph step");
     enqueue_search(true);
     const TravArgs a = trav_args(delta);
-    launch_pass(PASS_DENSITY, dp_, a, stream_, cfg_.warps_density);
-    launch_pass(PASS_FORCE, dp_, a, stream_, cfg_.warps_force);
-    launch_pass(PASS_SURFACE, dp_, a, stream_, cfg_.warps_surface);
+    {
+        NvtxRange rd("wcsph density pass");
+        launch_pass(PASS_DENSITY, dp_, a, stream_, cfg_.warps_density);
+    }
+    {
+        NvtxRange rf("wcsph force pass");
+        launch_pass(PASS_FORCE, dp_, a, stream_, cfg_.warps_force);
+    }
+    {
+        NvtxRange rs("wcsph surface + integrate pass");
+        launch_pass(PASS_SURFACE, dp_, a, stream_, cfg_.warps_surface);
+    }
 }
 
 int CUDASPHSimulator::launches_per_step() const {
@@ -386,6 +402,7 @@ void CUDASPHSimulator::update(float delta) {
 }
 
 void CUDASPHSimulator::step_n(int n, float delta) {
+    NvtxRange r("wcsph step_n (graph replay)");
     if (n <= 0) return;
     if (!graph_valid_ || graph_delta_ != delta) {
         invalidate_graph();

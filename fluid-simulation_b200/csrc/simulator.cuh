@@ -29,6 +29,16 @@ struct Error : std::runtime_error {
 void cuda_check(cudaError_t e, const char* what);
 #define WCSPH_CUDA(call) ::wcsph::cuda_check((call), #call)
 
+// Named NVTX range for the scope of the object (host side: the enqueue or
+// launch of a stage; a profiler attached to the process shows them, and they
+// cost nothing without one).
+struct NvtxRange {
+    explicit NvtxRange(const char* name);
+    ~NvtxRange();
+    NvtxRange(const NvtxRange&) = delete;
+    NvtxRange& operator=(const NvtxRange&) = delete;
+};
+
 // Device buffer with RAII.
 template <class T>
 struct DevBuf {
