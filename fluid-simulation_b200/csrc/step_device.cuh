@@ -419,16 +419,16 @@ __device__ __forceinline__ float cubic_grad_dr(float q, float r, const DevParams
 // Cubic spline divided by its factor 8/(pi h^3) (kernel.cuh:12-19), without
 // branches: 6q^3 - 6q^2 + 1 (q <= 1/2), 2(1-q)^3 (q <= 1), 0 beyond.
 __device__ __forceinline__ float cubic_shape(float q) {
-    const float t = 1.f - q;
-    const float inner = __fmaf_rn(6.f * q * q, q - 1.f, 1.f);
-    const float outer = 2.f * t * t * t;
+    const float t = __fsub_rn(1.f, q);
+    const float inner = __fmaf_rn(__fmul_rn(__fmul_rn(6.f, q), q), __fsub_rn(q, 1.f), 1.f);
+    const float outer = __fmul_rn(__fmul_rn(__fmul_rn(2.f, t), t), t);
     return q <= 0.5f ? inner : (q <= 1.f ? outer : 0.f);
 }
 
 // |r| / h from r^2 with one reciprocal square root; 0 for coincident points.
 __device__ __forceinline__ float q_of(float r2, float& rinv, const DevParams& P) {
     rinv = rsqrtf(fmaxf(r2, 1e-30f));
-    return r2 * rinv * P.inv_h;
+    return __fmul_rn(__fmul_rn(r2, rinv), P.inv_h);
 }
 
 // Fluid pair (i, candidate m of the staged chunk) contributions. v[] holds
@@ -445,36 +445,42 @@ __device__ __forceinline__ void fluid_pair(float* v, const HomeData& H, const Nb
     const float rx = H.x.x - d.x.x, ry = H.x.y - d.x.y, rz = H.x.z - d.x.z;
     if constexpr (KIND == PASS_DENSITY) {
         float rinv;
-        v[0] += cubic_shape(q_of(r2, rinv, P));
+        v[0] = __fadd_rn(v[0], cubic_shape(q_of(r2, rinv, P)));
     } else if constexpr (KIND == PASS_FORCE) {
         // spiky_grad / cubic_grad (kernel.cuh:22-51) as coefficients of r
+        // rounding written out (see finish_row): the sums must not depend on
+        // which kernel this is inlined into
         float rinv;
         const float q = q_of(r2, rinv, P);
-        const float t = 1.f - q;
-        const float kr = (q >= 1.e-9f && q <= 1.f) ? rinv * P.inv_h : 0.f;
-        const float sg = P.spiky_grad_factor * (t * t) * kr;
-        const float cg = P.cubic_grad_factor * (q <= 0.5f ? q * (3.f * q - 2.f) : -(t * t)) * kr;
-        const float c = (H.dpi + d.c) * sg;
-        v[0] -= c * rx; v[1] -= c * ry; v[2] -= c * rz;
-        const float cn = cg * d.b.w;
-        v[3] += rx * cn; v[4] += ry * cn; v[5] += rz * cn;
-        const float vr = (H.v.x - d.b.x) * rx + (H.v.y - d.b.y) * ry + (H.v.z - d.b.z) * rz;
-        const float s = __fdividef(vr * cn, r2 + P.visc_eps);
-        v[6] += s * rx; v[7] += s * ry; v[8] += s * rz;
+        const float t = __fsub_rn(1.f, q);
+        const float t2 = __fmul_rn(t, t);
+        const float kr = (q >= 1.e-9f && q <= 1.f) ? __fmul_rn(rinv, P.inv_h) : 0.f;
+        const float sg = __fmul_rn(__fmul_rn(P.spiky_grad_factor, t2), kr);
+        const float shape = q <= 0.5f ? __fmul_rn(q, __fmaf_rn(3.f, q, -2.f)) : -t2;
+        const float cg = __fmul_rn(__fmul_rn(P.cubic_grad_factor, shape), kr);
+        const float c = __fmul_rn(__fadd_rn(H.dpi, d.c), sg);
+        v[0] = __fmaf_rn(-c, rx, v[0]); v[1] = __fmaf_rn(-c, ry, v[1]); v[2] = __fmaf_rn(-c, rz, v[2]);
+        const float cn = __fmul_rn(cg, d.b.w);
+        v[3] = __fmaf_rn(rx, cn, v[3]); v[4] = __fmaf_rn(ry, cn, v[4]); v[5] = __fmaf_rn(rz, cn, v[5]);
+        const float vr = __fmaf_rn(__fsub_rn(H.v.z, d.b.z), rz,
+                                   __fmaf_rn(__fsub_rn(H.v.y, d.b.y), ry, __fmul_rn(__fsub_rn(H.v.x, d.b.x), rx)));
+        const float s = __fdividef(__fmul_rn(vr, cn), __fadd_rn(r2, P.visc_eps));
+        v[6] = __fmaf_rn(s, rx, v[6]); v[7] = __fmaf_rn(s, ry, v[7]); v[8] = __fmaf_rn(s, rz, v[8]);
     } else if constexpr (KIND == PASS_SURFACE) {
         // cohesion (kernel.cuh:53-63); pairs closer than 1e-3 are skipped
         const float4 nj = d.b;
         const float rho_j = d.c;
         float rinv;
         const float q = q_of(r2, rinv, P);
-        const float t = 1.f - q;
-        const float q3t3 = (q * q * q) * (t * t * t);
-        const float coh = P.cohesion_factor * (q <= 0.5f ? 2.f * q3t3 - 1.f / 64.f : (q <= 1.f ? q3t3 : 0.f));
-        const float inv = r2 > 1e-6f ? __fdividef(1.f, H.rho + rho_j) : 0.f;
-        const float cm = P.mass * coh * rinv;
-        v[0] += (cm * rx + H.n.x - nj.x) * inv;
-        v[1] += (cm * ry + H.n.y - nj.y) * inv;
-        v[2] += (cm * rz + H.n.z - nj.z) * inv;
+        const float t = __fsub_rn(1.f, q);
+        const float q3t3 = __fmul_rn(__fmul_rn(__fmul_rn(q, q), q), __fmul_rn(__fmul_rn(t, t), t));
+        const float shape = q <= 0.5f ? __fmaf_rn(2.f, q3t3, -1.f / 64.f) : (q <= 1.f ? q3t3 : 0.f);
+        const float coh = __fmul_rn(P.cohesion_factor, shape);
+        const float inv = r2 > 1e-6f ? __fdividef(1.f, __fadd_rn(H.rho, rho_j)) : 0.f;
+        const float cm = __fmul_rn(__fmul_rn(P.mass, coh), rinv);
+        v[0] = __fmaf_rn(__fsub_rn(__fmaf_rn(cm, rx, H.n.x), nj.x), inv, v[0]);
+        v[1] = __fmaf_rn(__fsub_rn(__fmaf_rn(cm, ry, H.n.y), nj.y), inv, v[1]);
+        v[2] = __fmaf_rn(__fsub_rn(__fmaf_rn(cm, rz, H.n.z), nj.z), inv, v[2]);
     } else if constexpr (KIND == PASS_ADJ_FORCE) {
         // pressure: a_i = -m sum_j A_ij F(r_ij), F(r) = g_s(|r|) r, A_ij = p_i/rho_i^2 + p_j/rho_j^2
         const u32 j = d.j;
@@ -537,11 +543,17 @@ __device__ __forceinline__ void boundary_pair(float* v, const HomeData& H, u32 b
     const float rx = H.x.x - xb.x, ry = H.x.y - xb.y, rz = H.x.z - xb.z;
     if constexpr (KIND == PASS_DENSITY) {
         float rinv;
-        v[0] += cubic_shape(q_of(r2, rinv, P)) * mb;
+        v[0] = __fmaf_rn(cubic_shape(q_of(r2, rinv, P)), mb, v[0]);
     } else if constexpr (KIND == PASS_FORCE) {
-        const float q = sqrtf(r2) * P.inv_h;
-        const float c = mb * (H.dpi + H.prs / P.rest_density2) * spiky_grad(q, P);
-        v[0] -= c * rx; v[1] -= c * ry; v[2] -= c * rz;
+        // rounding written out (see finish_row)
+        const float q = __fmul_rn(__fsqrt_rn(r2), P.inv_h);
+        float sgr = 0.f;   // spiky_grad (kernel.cuh:43-51)
+        if (!(q < 1.e-9f || q > 1.f)) {
+            const float t = __fsub_rn(1.f, q);
+            sgr = __fdiv_rn(__fmul_rn(__fmul_rn(P.spiky_grad_factor, t), t), __fmul_rn(P.h, __fmul_rn(q, P.h)));
+        }
+        const float c = __fmul_rn(__fmul_rn(mb, __fadd_rn(H.dpi, __fdiv_rn(H.prs, P.rest_density2))), sgr);
+        v[0] = __fmaf_rn(-c, rx, v[0]); v[1] = __fmaf_rn(-c, ry, v[1]); v[2] = __fmaf_rn(-c, rz, v[2]);
     } else if constexpr (KIND == PASS_ADJ_FORCE) {
         // a_i -= m_b B_i F(r_ib), B_i = p_i/rho_i^2 + p_i/rho0^2
         const float rl = sqrtf(r2);
