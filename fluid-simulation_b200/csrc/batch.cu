@@ -102,6 +102,7 @@ struct BatchSim {
     DevBuf<float> bmass;
     DevBuf<u64> btable, bckey;
     DevBuf<u32> bcstart, bcend;
+    BoundaryCells bcells;               // per-cell boundary candidate runs
     u32 btable_size = 0;
     int mask_words = 12;
     int nbr_width = 64;
@@ -131,6 +132,8 @@ struct BatchSim {
         a.bpos = bpos.ptr;
         a.bmass = bmass.ptr;
         a.boundary = HashView{btable.ptr, bcstart.ptr, bcend.ptr, btable_size ? btable_size - 1 : 0};
+        a.bcell = bcells.view();
+        a.bcx = bcells.x.ptr;
         a.mask = mask.ptr;
         a.mask_words = static_cast<u32>(mask_words);
         a.chunk = n < (1u << 18) ? 8u : 16u;
@@ -422,6 +425,7 @@ static void build_batch(BatchSim& B, const wcsph_params& p, const wcsph_batch_sc
         HashView bh{B.btable.ptr, B.bcstart.ptr, B.bcend.ptr, B.btable_size - 1};
         launch_boundary_mass(B.dp, B.bpos.ptr, nbb, bh, B.bmass.ptr, s, B.bckey.ptr);
         WCSPH_CUDA(cudaGetLastError());
+        build_boundary_cells(B.bcells, bh, B.btable_size, nbb, B.bpos.ptr, B.bmass.ptr, true, B.st.ptr, s);
         WCSPH_CUDA(cudaStreamSynchronize(s));
     }
     B.check_errors();

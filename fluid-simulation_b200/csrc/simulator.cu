@@ -252,6 +252,7 @@ void CUDASPHSimulator::init_boundary(const float* bpos_host) {
     HashView bh{btable_.ptr, bcstart_.ptr, bcend_.ptr, btable_size_ - 1};
     launch_boundary_mass(dp_, bpos_.ptr, nb, bh, bmass_.ptr, stream_);
     WCSPH_CUDA(cudaGetLastError());
+    build_boundary_cells(bcells_, bh, btable_size_, nb, bpos_.ptr, bmass_.ptr, false, st_.ptr, stream_);
     WCSPH_CUDA(cudaStreamSynchronize(stream_));
     check_device_errors();
 }
@@ -292,6 +293,8 @@ TravArgs CUDASPHSimulator::trav_args(float delta) {
     a.bpos = bpos_.ptr;
     a.bmass = bmass_.ptr;
     a.boundary = HashView{btable_.ptr, bcstart_.ptr, bcend_.ptr, btable_size_ ? btable_size_ - 1 : 0};
+    a.bcell = bcells_.view();
+    a.bcx = bcells_.x.ptr;
     a.mask = mask_.ptr;
     a.mask_words = static_cast<u32>(cfg_.mask_words);
     a.chunk = effective_chunk(cfg_, n_);
@@ -482,6 +485,8 @@ void CUDASPHSimulator::set_params(const wcsph_params& p) {
         HashView bh{btable_.ptr, bcstart_.ptr, bcend_.ptr, btable_size_ - 1};
         launch_boundary_mass(dp_, bpos_.ptr, nb_, bh, bmass_.ptr, stream_);
         WCSPH_CUDA(cudaGetLastError());
+        // the per-cell candidate runs carry copies of the masses
+        build_boundary_cells(bcells_, bh, btable_size_, nb_, bpos_.ptr, bmass_.ptr, false, st_.ptr, stream_);
     }
 }
 

@@ -73,6 +73,23 @@ struct DevBuf {
     size_t bytes() const { return count * sizeof(T); }
 };
 
+// Boundary candidates per cell (boundary_cells.cu): for every cell within one
+// cell of an occupied boundary cell (cell size h), the boundary particles of
+// its 27 neighbour cells in the (dx, dy, dz) order of the boundary loops, as
+// (x, y, z, mass) runs [start, end) of x, found through the hash `table`.
+struct BoundaryCells {
+    DevBuf<u64> table;
+    DevBuf<u32> start, end;
+    DevBuf<float4> x;
+    u32 size = 0;   // 0: not built (the passes then look the 27 cells up themselves)
+    HashView view() const { return HashView{table.ptr, start.ptr, end.ptr, size ? size - 1 : 0}; }
+};
+// Builds bc from the boundary hash bh (bsize slots) of nb sorted boundary
+// particles; batch: keys are (scene, cell). Leaves bc empty where the 32-bit
+// run offsets would not suffice. Synchronises the stream.
+void build_boundary_cells(BoundaryCells& bc, const HashView& bh, u32 bsize, u32 nb, const float4* bpos,
+                          const float* bmass, bool batch, DevState* st, cudaStream_t s);
+
 DevParams make_dev_params(const wcsph_params& p);
 DevBox make_dev_box(const wcsph_box& b);
 void validate_params(const wcsph_params& p);
@@ -230,6 +247,7 @@ private:
     DevBuf<u64> btable_;
     DevBuf<u32> bcstart_, bcend_;
     uint32_t btable_size_ = 0;
+    BoundaryCells bcells_;
 
     // CUDA graph of one step, keyed by the requested delta
     cudaGraphExec_t graph_exec_ = nullptr;

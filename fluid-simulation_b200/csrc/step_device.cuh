@@ -427,7 +427,7 @@ __device__ __forceinline__ float cubic_shape(float q) {
 
 // |r| / h from r^2 with one reciprocal square root; 0 for coincident points.
 __device__ __forceinline__ float q_of(float r2, float& rinv, const DevParams& P) {
-    rinv = rsqrtf(fmaxf(r2, 1e-30f));
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(rinv) : "f"(fmaxf(r2, 1e-30f)));
     return __fmul_rn(__fmul_rn(r2, rinv), P.inv_h);
 }
 
@@ -537,9 +537,8 @@ __device__ __forceinline__ void fluid_pair(float* v, const HomeData& H, const Nb
 //   DENSITY v0 = sum m_b W / cubic_factor; FORCE v0..2 = boundary pressure accel;
 //   ADJ_FORCE v0..2 = dL/dx_i, v3 = boundary pressure-coefficient term; ADJ_DENSITY v0..2 = dL/dx_i
 template <int KIND>
-__device__ __forceinline__ void boundary_pair(float* v, const HomeData& H, u32 b, float4 xb, float r2,
-                                              const DevParams& P, const TravArgs& a) {
-    const float mb = ro_ld(a.bmass + b);
+__device__ __forceinline__ void boundary_pair_m(float* v, const HomeData& H, float mb, float4 xb, float r2,
+                                                const DevParams& P) {
     const float rx = H.x.x - xb.x, ry = H.x.y - xb.y, rz = H.x.z - xb.z;
     if constexpr (KIND == PASS_DENSITY) {
         float rinv;
@@ -570,6 +569,30 @@ __device__ __forceinline__ void boundary_pair(float* v, const HomeData& H, u32 b
     } else if constexpr (KIND == PASS_ADJ_DENSITY) {
         const float c = mb * H.rb * cubic_grad(sqrtf(r2) * P.inv_h, P);
         v[0] += c * rx; v[1] += c * ry; v[2] += c * rz;
+    }
+}
+template <int KIND>
+__device__ __forceinline__ void boundary_pair(float* v, const HomeData& H, u32 b, float4 xb, float r2,
+                                              const DevParams& P, const TravArgs& a) {
+    boundary_pair_m<KIND>(v, H, ro_ld(a.bmass + b), xb, r2, P);
+}
+
+// Boundary key of cell c (cell size h) of the scene.
+template <bool BATCH>
+__device__ __forceinline__ u64 boundary_cell_key(int3 c, u32 scene) {
+    if constexpr (BATCH) return pack_cell_batch(scene, offset_coord(c.x), offset_coord(c.y), offset_coord(c.z));
+    else return pack_cell(c);
+}
+
+// Run [start, end) of the per-cell boundary candidates of cell key pk
+// (empty when pk is not within one cell of any boundary particle).
+template <bool BATCH>
+__device__ __forceinline__ void boundary_run(const TravArgs& a, u64 pk, u32& start, u32& end) {
+    const u32 slot = find_slot<BATCH>(a.bcell.table, a.bcell.tmask, pk);
+    start = end = 0;
+    if (slot != EMPTY_CELL) {
+        start = ro_ld(a.bcell.cstart + slot);
+        end = ro_ld(a.bcell.cend + slot);
     }
 }
 
@@ -844,6 +867,63 @@ __device__ __forceinline__ u32 boundary_pair_run(const WarpView<KIND>& S, const 
     return c;
 }
 
+// Boundary pairs of rows [0, nh) from per-cell candidate runs: rows
+// [0, split) against run A = [sa, sa + la) of bcx, later rows against run
+// B = [sb, sb + lb) (the second cell of an x-pair). Segmented like
+// boundary_pair_run; returns the run length and, for row k = lane, its item
+// range [lo, hi).
+template <int KIND>
+__device__ __forceinline__ u32 boundary_cells_run(const WarpView<KIND>& S, const DevParams& P, const TravArgs& a,
+                                                  u32 nh, u32 i0, u32 split, u32 sa, u32 la, u32 sb, u32 lb,
+                                                  u32& lo, u32& hi) {
+    constexpr int NFB = KindCfg<KIND>::nfb;
+    const u32 lane = lane_id();
+    const u32 na = split * la;
+    const u32 total = na + (nh - split) * lb;
+    lo = lane < split ? lane * la : na + (min(lane, nh) - split) * lb;
+    hi = lo + (lane < nh ? (lane < split ? la : lb) : 0u);
+    if (total == 0) return 0;
+    const u32 c = ((total + 31u) >> 5) | 1u;
+    u32 p = lane * c;
+    const u32 e = min(p + c, total);
+    if (p < e) {
+        u32 k, m;
+        if (p < na) {
+            k = p / la;
+            m = p - k * la;
+        } else {
+            const u32 q = p - na;
+            k = split + q / lb;
+            m = q - (k - split) * lb;
+        }
+        u32 len = k < split ? la : lb;
+        const float4* run = a.bcx + (k < split ? sa : sb);
+        HomeData H = load_home<KIND>(a, i0 + k);
+        float v[NFB];
+#pragma unroll
+        for (int f = 0; f < NFB; ++f) v[f] = 0.f;
+        for (;;) {
+            const float4 xb = ro_ld(run + m);
+            const float r2 = dist2(H.x, xb);
+            if (r2 <= P.h2) boundary_pair_m<KIND>(v, H, xb.w, xb, r2, P);
+            ++p;
+            if (++m == len || p == e) {
+                store_partial<NFB>(S.part, lane + k, v);
+                if (p == e) break;
+#pragma unroll
+                for (int f = 0; f < NFB; ++f) v[f] = 0.f;
+                m = 0;
+                ++k;
+                len = k < split ? la : lb;
+                run = a.bcx + (k < split ? sa : sb);
+                H = load_home<KIND>(a, i0 + k);
+            }
+        }
+    }
+    __syncwarp();
+    return c;
+}
+
 // Per-row epilogue of a pass: the sums res (fluid) and resb (boundary) of
 // particle i become its fields; the surface pass integrates and adds to
 // the warp's CFL / metric reductions. The rounding of every step is written
@@ -1007,6 +1087,16 @@ template <int KIND, bool BATCH>
 __device__ __forceinline__ void boundary_row(const DevParams& P, const TravArgs& a, const HomeData& H, u32 scene,
                                              float* resb) {
     const int3 c = cell_of(H.x, P.h);
+    if (a.bcell.table != nullptr) {   // the cell's candidates, gathered in the same order
+        u32 t, e;
+        boundary_run<BATCH>(a, boundary_cell_key<BATCH>(c, scene), t, e);
+        for (; t < e; ++t) {
+            const float4 xb = ro_ld(a.bcx + t);
+            const float r2 = dist2(H.x, xb);
+            if (r2 <= P.h2) boundary_pair_m<KIND>(resb, H, xb.w, xb, r2, P);
+        }
+        return;
+    }
     for (int dx = -1; dx <= 1; ++dx)
         for (int dy = -1; dy <= 1; ++dy)
             for (int dz = -1; dz <= 1; ++dz) {
@@ -1273,8 +1363,23 @@ __device__ __forceinline__ void cell_pass_chunk(const DevParams& P, const TravAr
             // boundary-cell neighbourhoods (cell size h, R = 1,
             // for_boundary_neighbors common.cuh:153-178)
             u32 MB = 0, nbc = 0;
+            // density with per-cell boundary candidates (cell size h): the
+            // runs of the unit's home cells (A, and B of an x-pair)
+            const bool use_cells = KIND == PASS_DENSITY && a.bcell.table != nullptr && P.cell_size == P.h;
+            u32 bra = 0, bla = 0, brb = 0, blb = 0;
+            if (use_cells && a.nb > 0) {
+                u32 s0 = 0, s1 = 0;
+                if (lane < (pair ? 2u : 1u)) {
+                    const int3 hc = cell_of(a.pos[home_start + (lane ? nA : 0u)], P.h);
+                    boundary_run<BATCH>(a, boundary_cell_key<BATCH>(hc, scene), s0, s1);
+                }
+                bra = __shfl_sync(FULL, s0, 0);
+                bla = __shfl_sync(FULL, s1, 0) - bra;
+                brb = __shfl_sync(FULL, s0, 1);
+                blb = __shfl_sync(FULL, s1, 1) - brb;
+            }
             if constexpr (C::boundary) {
-                if (a.nb > 0) {
+                if (a.nb > 0 && !use_cells) {
                     int lo[3] = {INT_MAX, INT_MAX, INT_MAX}, hi[3] = {INT_MIN, INT_MIN, INT_MIN};
                     for (u32 k = lane; k < n_home; k += 32) {
                         const int3 c = cell_of(a.pos[home_start + k], P.h);
@@ -1428,7 +1533,12 @@ __device__ __forceinline__ void cell_pass_chunk(const DevParams& P, const TravAr
                 }
 
                 // boundary candidates (density and pressure passes)
-                if constexpr (C::boundary) {
+                if (use_cells) {
+                    u32 blo, bhi;
+                    const u32 c = boundary_cells_run<KIND>(S, P, a, nh, i0, min(hm.split, nh), bra, bla, brb, blb,
+                                                           blo, bhi);
+                    if (c) combine<NFB>(S.part, resb, act, blo, bhi, c, lane);
+                } else if constexpr (C::boundary) {
                     for (u32 c0 = 0; c0 < MB; c0 += BCAND_CAP) {
                         const u32 len = min(BCAND_CAP, MB - c0);
                         expand(S.bcand, S.bstart, S.bpref, nbc, c0, len);

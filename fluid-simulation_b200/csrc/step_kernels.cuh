@@ -72,6 +72,10 @@ struct TravArgs {
     const float4* bpos;
     const float* bmass;
     HashView boundary;
+    // per-cell boundary candidates (runs of (x, y, z, mass) in bcx; table
+    // nullptr: not built, the passes look the 27 boundary cells up)
+    HashView bcell;
+    const float4* bcx;
     // neighbour bitmasks
     u32* mask;
     u32 mask_words;           // words per particle (candidate cap = 32*mask_words)
