@@ -103,6 +103,7 @@ struct BatchSim {
     DevBuf<u64> btable, bckey;
     DevBuf<u32> bcstart, bcend;
     BoundaryCells bcells;               // per-cell boundary candidate runs
+    DevBuf<uint4> bmask;                // boundary hit masks
     u32 btable_size = 0;
     int mask_words = 12;
     int nbr_width = 64;
@@ -134,6 +135,7 @@ struct BatchSim {
         a.boundary = HashView{btable.ptr, bcstart.ptr, bcend.ptr, btable_size ? btable_size - 1 : 0};
         a.bcell = bcells.view();
         a.bcx = bcells.x.ptr;
+        a.bmask = (bcells.size && mask_words >= 4 && dp.cell_size == dp.h) ? bmask.ptr : nullptr;
         a.mask = mask.ptr;
         a.mask_words = static_cast<u32>(mask_words);
         a.chunk = n < (1u << 18) ? 8u : 16u;
@@ -426,6 +428,7 @@ static void build_batch(BatchSim& B, const wcsph_params& p, const wcsph_batch_sc
         launch_boundary_mass(B.dp, B.bpos.ptr, nbb, bh, B.bmass.ptr, s, B.bckey.ptr);
         WCSPH_CUDA(cudaGetLastError());
         build_boundary_cells(B.bcells, bh, B.btable_size, nbb, B.bpos.ptr, B.bmass.ptr, true, B.st.ptr, s);
+        if (B.bcells.size) B.bmask.alloc(B.n);
         WCSPH_CUDA(cudaStreamSynchronize(s));
     }
     B.check_errors();

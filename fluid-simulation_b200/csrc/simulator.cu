@@ -253,6 +253,7 @@ void CUDASPHSimulator::init_boundary(const float* bpos_host) {
     launch_boundary_mass(dp_, bpos_.ptr, nb, bh, bmass_.ptr, stream_);
     WCSPH_CUDA(cudaGetLastError());
     build_boundary_cells(bcells_, bh, btable_size_, nb, bpos_.ptr, bmass_.ptr, false, st_.ptr, stream_);
+    if (bcells_.size) bmask_.alloc(n_);
     WCSPH_CUDA(cudaStreamSynchronize(stream_));
     check_device_errors();
 }
@@ -295,6 +296,9 @@ TravArgs CUDASPHSimulator::trav_args(float delta) {
     a.boundary = HashView{btable_.ptr, bcstart_.ptr, bcend_.ptr, btable_size_ ? btable_size_ - 1 : 0};
     a.bcell = bcells_.view();
     a.bcx = bcells_.x.ptr;
+    // the density pass writes the masks where it reads the runs (cell size h);
+    // they are built in its bit-matrix scratch (4 words per row)
+    a.bmask = (bcells_.size && cfg_.mask_words >= 4 && dp_.cell_size == dp_.h) ? bmask_.ptr : nullptr;
     a.mask = mask_.ptr;
     a.mask_words = static_cast<u32>(cfg_.mask_words);
     a.chunk = effective_chunk(cfg_, n_);

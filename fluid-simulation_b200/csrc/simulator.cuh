@@ -248,6 +248,7 @@ private:
     DevBuf<u32> bcstart_, bcend_;
     uint32_t btable_size_ = 0;
     BoundaryCells bcells_;
+    DevBuf<uint4> bmask_;   // boundary hit masks (per-cell runs)
 
     // CUDA graph of one step, keyed by the requested delta
     cudaGraphExec_t graph_exec_ = nullptr;

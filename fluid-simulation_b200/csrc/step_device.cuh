@@ -872,10 +872,12 @@ __device__ __forceinline__ u32 boundary_pair_run(const WarpView<KIND>& S, const 
 // B = [sb, sb + lb) (the second cell of an x-pair). Segmented like
 // boundary_pair_run; returns the run length and, for row k = lane, its item
 // range [lo, hi).
+// masks (density, a.bmask): hit m < 128 of row k also sets bit m of
+// S.aux[4k .. 4k + 3], which the caller zeroes before and stores after.
 template <int KIND>
 __device__ __forceinline__ u32 boundary_cells_run(const WarpView<KIND>& S, const DevParams& P, const TravArgs& a,
                                                   u32 nh, u32 i0, u32 split, u32 sa, u32 la, u32 sb, u32 lb,
-                                                  u32& lo, u32& hi) {
+                                                  u32& lo, u32& hi, bool masks = false) {
     constexpr int NFB = KindCfg<KIND>::nfb;
     const u32 lane = lane_id();
     const u32 na = split * la;
@@ -905,7 +907,10 @@ __device__ __forceinline__ u32 boundary_cells_run(const WarpView<KIND>& S, const
         for (;;) {
             const float4 xb = ro_ld(run + m);
             const float r2 = dist2(H.x, xb);
-            if (r2 <= P.h2) boundary_pair_m<KIND>(v, H, xb.w, xb, r2, P);
+            if (r2 <= P.h2) {
+                boundary_pair_m<KIND>(v, H, xb.w, xb, r2, P);
+                if (masks && m < 128u) atomicOr(S.aux + 4u * k + (m >> 5), 1u << (m & 31u));
+            }
             ++p;
             if (++m == len || p == e) {
                 store_partial<NFB>(S.part, lane + k, v);
@@ -1085,11 +1090,25 @@ __device__ __forceinline__ void spill_row(const DevParams& P, const TravArgs& a,
 // (common.cuh:153-178) visits them, one particle after the other.
 template <int KIND, bool BATCH>
 __device__ __forceinline__ void boundary_row(const DevParams& P, const TravArgs& a, const HomeData& H, u32 scene,
-                                             float* resb) {
+                                             float* resb, u32 i) {
     const int3 c = cell_of(H.x, P.h);
     if (a.bcell.table != nullptr) {   // the cell's candidates, gathered in the same order
         u32 t, e;
         boundary_run<BATCH>(a, boundary_cell_key<BATCH>(c, scene), t, e);
+        if (a.bmask != nullptr && e - t <= 128u) {
+            // the density pass of this step marked the candidates within h
+            // (same positions, same predicate): visit those, in run order
+            const uint4 mk = ro_ld(a.bmask + i);
+            const u32 words[4] = {mk.x, mk.y, mk.z, mk.w};
+#pragma unroll
+            for (u32 w = 0; w < 4; ++w) {
+                for (u32 bits = words[w]; bits; bits &= bits - 1) {
+                    const float4 xb = ro_ld(a.bcx + t + 32u * w + (__ffs(bits) - 1));
+                    boundary_pair_m<KIND>(resb, H, xb.w, xb, dist2(H.x, xb), P);
+                }
+            }
+            return;
+        }
         for (; t < e; ++t) {
             const float4 xb = ro_ld(a.bcx + t);
             const float r2 = dist2(H.x, xb);
@@ -1168,7 +1187,7 @@ __device__ __forceinline__ void list_rows(const DevParams& P, const TravArgs& a,
             }
         }
         if constexpr (C::boundary) {
-            if (a.nb > 0) boundary_row<KIND, BATCH>(P, a, H, scene, resb);
+            if (a.nb > 0) boundary_row<KIND, BATCH>(P, a, H, scene, resb, i);
         }
     }
     if (act) finish_row<KIND, BATCH>(P, a, i, res, resb, 0u, scene, dt, np_dt, red_max, red_speed, red_speed2);
@@ -1534,10 +1553,18 @@ __device__ __forceinline__ void cell_pass_chunk(const DevParams& P, const TravAr
 
                 // boundary candidates (density and pressure passes)
                 if (use_cells) {
+                    const bool masks = a.bmask != nullptr;
+                    if (masks) {
+                        for (u32 w = lane; w < 4u * nh; w += 32) S.aux[w] = 0u;
+                        __syncwarp();
+                    }
                     u32 blo, bhi;
                     const u32 c = boundary_cells_run<KIND>(S, P, a, nh, i0, min(hm.split, nh), bra, bla, brb, blb,
-                                                           blo, bhi);
+                                                           blo, bhi, masks);
                     if (c) combine<NFB>(S.part, resb, act, blo, bhi, c, lane);
+                    if (masks && act)
+                        a.bmask[i] = make_uint4(S.aux[4 * lane], S.aux[4 * lane + 1], S.aux[4 * lane + 2],
+                                                S.aux[4 * lane + 3]);
                 } else if constexpr (C::boundary) {
                     for (u32 c0 = 0; c0 < MB; c0 += BCAND_CAP) {
                         const u32 len = min(BCAND_CAP, MB - c0);
