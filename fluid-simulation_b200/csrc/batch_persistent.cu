@@ -154,7 +154,7 @@ __global__ void __launch_bounds__(PTHREADS, 3) persistent_ensemble_kernel(const 
         if (a.nbr) {
             for (u32 g0 = claim(ps.barrier + WORK_FORCE); g0 < ngroups; g0 = claim(ps.barrier + WORK_FORCE))
                 for (u32 g = g0; g < min(g0 + CLAIM, ngroups); ++g)
-                    list_rows<PASS_FORCE, true>(P, a, g * rows, min(rows, n - g * rows), 0.f, 0.f, rm, rs, rs2);
+                    list_rows<PASS_FORCE, true, 1>(P, a, g * rows, min(rows, n - g * rows), 0.f, 0.f, rm, rs, rs2);
         } else {
             const WarpView<PASS_FORCE> S = warp_view<PASS_FORCE>(a, smem, warp);
             for (u32 c0 = claim(ps.barrier + WORK_FORCE); c0 < nchunks; c0 = claim(ps.barrier + WORK_FORCE))
@@ -166,7 +166,7 @@ __global__ void __launch_bounds__(PTHREADS, 3) persistent_ensemble_kernel(const 
         if (a.nbr) {
             for (u32 g0 = claim(ps.barrier + WORK_SURFACE); g0 < ngroups; g0 = claim(ps.barrier + WORK_SURFACE))
                 for (u32 g = g0; g < min(g0 + CLAIM, ngroups); ++g)
-                    list_rows<PASS_SURFACE, true>(P, a, g * rows, min(rows, n - g * rows), dt, np_dt, rm, rs, rs2);
+                    list_rows<PASS_SURFACE, true, 2>(P, a, g * rows, min(rows, n - g * rows), dt, np_dt, rm, rs, rs2);
         } else {
             const WarpView<PASS_SURFACE> S = warp_view<PASS_SURFACE>(a, smem, warp);
             for (u32 c0 = claim(ps.barrier + WORK_SURFACE); c0 < nchunks; c0 = claim(ps.barrier + WORK_SURFACE))

@@ -1138,7 +1138,12 @@ __device__ __forceinline__ void boundary_row(const DevParams& P, const TravArgs&
 // particles [i0, i0 + nh) of its chunk, whatever their cells; lane k sums
 // row k's list in order (the reference's per-particle order), so a row's
 // sums do not depend on which particles share its warp.
-template <int KIND, bool BATCH>
+// DEPTH: neighbour records in flight per lane while a pair is summed (1, or
+// 2 where the registers are there anyway: the persistent ensemble kernel
+// runs at the density pass's register budget, with fewer resident warps than
+// the list kernels; its surface phase gains from the second record in flight,
+// its force phase does not).
+template <int KIND, bool BATCH, int DEPTH = 1>
 __device__ __forceinline__ void list_rows(const DevParams& P, const TravArgs& a, u32 i0, u32 nh, float dt,
                                           float np_dt, float& red_max, float& red_speed, float& red_speed2) {
     using C = KindCfg<KIND>;
@@ -1171,19 +1176,39 @@ __device__ __forceinline__ void list_rows(const DevParams& P, const TravArgs& a,
             // slot t of row i at nbr[t * n + i]; the next neighbour's records
             // and the index after it are in flight while a pair is summed
             const size_t stride = a.n;
-            const u32* lst = a.nbr + i + stride;
-            Nbr d = fetch_j<KIND>(a, ro_ld(a.nbr + i));
-            u32 jn = cnt > 1 ? ro_ld(lst) : 0u;
-            lst += stride;
-            for (u32 t = 0; t < cnt; ++t) {
-                Nbr dn = d;
-                if (t + 1 < cnt) dn = fetch_j<KIND>(a, jn);
-                if (t + 2 < cnt) {
-                    jn = ro_ld(lst);
-                    lst += stride;
+            if constexpr (DEPTH == 1) {
+                const u32* lst = a.nbr + i + stride;
+                Nbr d = fetch_j<KIND>(a, ro_ld(a.nbr + i));
+                u32 jn = cnt > 1 ? ro_ld(lst) : 0u;
+                lst += stride;
+                for (u32 t = 0; t < cnt; ++t) {
+                    Nbr dn = d;
+                    if (t + 1 < cnt) dn = fetch_j<KIND>(a, jn);
+                    if (t + 2 < cnt) {
+                        jn = ro_ld(lst);
+                        lst += stride;
+                    }
+                    fluid_pair<KIND>(res, H, d, dist2(H.x, d.x), P, a);
+                    d = dn;
                 }
-                fluid_pair<KIND>(res, H, d, dist2(H.x, d.x), P, a);
-                d = dn;
+            } else {
+                const u32* lst = a.nbr + i;
+                Nbr d0 = fetch_j<KIND>(a, ro_ld(lst));
+                Nbr d1 = d0;
+                if (cnt > 1) d1 = fetch_j<KIND>(a, ro_ld(lst + stride));
+                u32 jn = cnt > 2 ? ro_ld(lst + 2 * stride) : 0u;
+                lst += 3 * stride;
+                for (u32 t = 0; t < cnt; ++t) {
+                    Nbr d2 = d1;
+                    if (t + 2 < cnt) d2 = fetch_j<KIND>(a, jn);
+                    if (t + 3 < cnt) {
+                        jn = ro_ld(lst);
+                        lst += stride;
+                    }
+                    fluid_pair<KIND>(res, H, d0, dist2(H.x, d0.x), P, a);
+                    d0 = d1;
+                    d1 = d2;
+                }
             }
         }
         if constexpr (C::boundary) {
