@@ -275,6 +275,7 @@ def run_ours(args, world, rank, local, dist):
     if world == 1 and not args.no_extras:
         extras["batched"] = bench_batched(args)
         extras["rollout"] = bench_rollout()
+        extras["mesh_obstacle"] = bench_mesh()
     if rank != 0:
         return None
     peak, peak_kind = measured_peaks()
@@ -345,6 +346,31 @@ def bench_batched(args, n_scenes: int = 256, steps: int = 500):
     out["sequential_value"] = total * steps / seq_s
     out["gain"] = out["value"] / out["sequential_value"]
     out["launches"] = {"persistent": 1, "per_stage": 14 * steps, "sequential": 14 * n_scenes * steps}
+    return out
+
+
+def bench_mesh(steps: int = 200, warmup: int = 10):
+    """The mesh-obstacle scene (393,216 particles, walls and a sampled sphere,
+    CFL-adaptive dt): device time per step over `steps` steps."""
+    import torch
+
+    import wcsph
+
+    pre = wcsph.preset("mesh_obstacle")
+    sim = pre.simulator()
+    stream = torch.cuda.ExternalStream(sim.stream_handle())
+    sim.step_n(warmup, pre.info.delta)
+    sim.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    sim.step_n(steps, pre.info.delta)
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    out = {"particles": pre.info.fluid_n, "boundary_particles": pre.info.boundary_n, "steps": steps,
+           "ms_per_step": ms, "value": pre.info.fluid_n / (ms * 1e-3), "unit": METRIC, "last_dt": sim.last_dt()[0]}
+    sim.close()
     return out
 
 
