@@ -319,10 +319,8 @@ def bench_batched(args, n_scenes: int = 256, steps: int = 500):
     stepped one after another through the single-scene path."""
     import wcsph
 
-    pres = [wcsph.preset_ensemble(args.seed + 1, k) for k in range(n_scenes)]
+    pres, specs = ensemble_scenes(args, n_scenes)
     total = sum(p.info.fluid_n for p in pres)
-    specs = [wcsph.BatchSceneSpec(fluid_pos=s.pos, box=s.box, gravity=tuple(s.params.gravity),
-                                  viscosity=s.params.viscosity, boundary_pos=s.bpos) for s in pres]
     out = {"scenes": n_scenes, "particles": total, "steps": steps, "unit": METRIC}
     for mode, persistent in (("persistent", True), ("per_stage", False)):
         b = wcsph.BatchSimulator(pres[0].params, specs)
@@ -347,6 +345,28 @@ def bench_batched(args, n_scenes: int = 256, steps: int = 500):
     out["gain"] = out["value"] / out["sequential_value"]
     out["launches"] = {"persistent": 1, "per_stage": 14 * steps, "sequential": 14 * n_scenes * steps}
     return out
+
+
+def ensemble_scenes(args, n_scenes: int = 256):
+    import wcsph
+
+    pres = [wcsph.preset_ensemble(args.seed + 1, k) for k in range(n_scenes)]
+    specs = [wcsph.BatchSceneSpec(fluid_pos=s.pos, box=s.box, gravity=tuple(s.params.gravity),
+                                  viscosity=s.params.viscosity, boundary_pos=s.bpos) for s in pres]
+    return pres, specs
+
+
+def ensemble_steps(args, k: int):
+    """The batched ensemble's per-stage launches for 3 + k steps, untimed (a
+    short, bounded workload for a launch-list capture)."""
+    import wcsph
+
+    pres, specs = ensemble_scenes(args)
+    b = wcsph.BatchSimulator(pres[0].params, specs)
+    b.set_persistent(False)
+    b.step_n(3 + k, 1e-3)
+    b.metrics()   # reads back, so the steps have finished
+    b.close()
 
 
 def bench_mesh(steps: int = 200, warmup: int = 10):
@@ -420,7 +440,12 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the ensemble and rollout measurements")
     ap.add_argument("--cpu-budget", type=float, default=15.0)
+    ap.add_argument("--ensemble-only", type=int, default=0, metavar="K",
+                    help="profiling entry: build the 256-scene ensemble, run 3 + K per-stage steps, print nothing")
     args = ap.parse_args()
+    if args.ensemble_only:
+        ensemble_steps(args, args.ensemble_only)
+        return
     args.warmup = max(args.warmup, 3)
     world, rank, local, dist = dist_setup()
     try:

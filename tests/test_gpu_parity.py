@@ -90,6 +90,16 @@ def test_cell_size_multipliers(mult):
     check_step(p, bx, pos, np.zeros_like(pos), bpos, 1e-3)
 
 
+@pytest.mark.parametrize("words", [2, 3])
+def test_walls_without_boundary_hit_masks(words):
+    # below 4 bit-matrix words the density pass keeps no boundary hit masks:
+    # the force pass scans each particle's whole per-cell boundary run (and
+    # most cells take the chunked path of an over-full bit matrix)
+    p, bx, pos, bpos = dam_break_scene(dims=(12, 14, 10))
+    vel = wcsph.make_velocities(pos.shape[0], 0.3, seed=5)
+    check_step(p, bx, pos, vel, bpos, 1e-3, config={"mask_words": words})
+
+
 def test_reference_constants_origin_centred_tilted_box():
     # reference defaults (r = 0.02, k = 0.1, nu = 0.001); the lattice straddles
     # the origin so cell coordinates change sign (63-bit keys), box rotated 0.1 rad
