@@ -40,12 +40,13 @@ __global__ void __launch_bounds__(WPB * 32, KindCfg<KIND>::min_warps / WPB) cell
 
 
 // Resident warps per SM the register allocation of the list kernels must
-// allow (36 -> 56 registers, 40 -> 48). The force pass fits 56 without
-// spilling (36 resident warps hide more of its gathers than 32 at 64
-// registers did); at 48 it spills.
+// allow (36 -> 56 registers, 48 -> 42). Both passes wait on neighbour
+// gathers, so resident warps pay as long as nothing spills: the force pass
+// fits 56 registers (36 warps; at 48 it spills), the surface pass 40 (50
+// warps with two-warp blocks, against 40 at the 47 it takes when allowed 48).
 template <int KIND>
 struct ListCfg {
-    static constexpr int min_warps = KIND == PASS_FORCE ? 36 : 40;
+    static constexpr int min_warps = KIND == PASS_FORCE ? 36 : 48;
 };
 
 // Force / surface pass over the neighbour lists written by the density pass.
