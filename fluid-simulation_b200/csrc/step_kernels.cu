@@ -40,18 +40,20 @@ __global__ void __launch_bounds__(WPB * 32, KindCfg<KIND>::min_warps / WPB) cell
 
 
 // Resident warps per SM the register allocation of the list kernels must
-// allow (36 -> 56 registers, 48 -> 42). Both passes wait on neighbour
-// gathers, so resident warps pay as long as nothing spills: the force pass
-// fits 56 registers (36 warps; at 48 it spills), the surface pass 40 (50
-// warps with two-warp blocks, against 40 at the 47 it takes when allowed 48).
-template <int KIND>
+// allow (32 -> 64 registers, 36 -> 56, 40 -> 48, 48 -> 42). Both passes wait
+// on neighbour gathers, so resident warps pay as long as nothing spills: the
+// single-scene force pass fits 56 registers (36 warps; at 48 it spills), the
+// surface pass 40 (50 warps with two-warp blocks, against 40 at the 47 it
+// takes when allowed 48). The batched passes, with the scene lookups, would
+// spill at those caps and keep 64 / 48.
+template <int KIND, bool BATCH>
 struct ListCfg {
-    static constexpr int min_warps = KIND == PASS_FORCE ? 36 : 48;
+    static constexpr int min_warps = BATCH ? (KIND == PASS_FORCE ? 32 : 40) : (KIND == PASS_FORCE ? 36 : 48);
 };
 
 // Force / surface pass over the neighbour lists written by the density pass.
 template <int KIND, int WPB, bool BATCH>
-__global__ void __launch_bounds__(WPB * 32, ListCfg<KIND>::min_warps / WPB) list_pass_kernel(const DevParams P,
+__global__ void __launch_bounds__(WPB * 32, ListCfg<KIND, BATCH>::min_warps / WPB) list_pass_kernel(const DevParams P,
                                                                                           const TravArgs a) {
     if (a.st->error_flags & ERR_LOOKBACK_TIMEOUT) return;   // no sorted state this step (reorder skipped)
     const u32 lane = lane_id();
