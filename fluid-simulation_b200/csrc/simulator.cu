@@ -342,8 +342,10 @@ void CUDASPHSimulator::enqueue_search(bool keys_from_state) {
 
 void CUDASPHSimulator::enqueue_keys() {
     const u32 n = n_;
-    // few blocks: each flushes its histograms / bounds with global atomics on shared addresses
-    const u32 blocks = std::min<u32>((n + 255) / 256, 296);
+    // four blocks per SM: each flushes its histograms / bounds with global
+    // atomics on shared addresses, so fewer blocks mean fewer atomics, more
+    // blocks more loads in flight (two per SM: 4 us more for the histograms)
+    const u32 blocks = std::min<u32>((n + 255) / 256, 592);
     keys_bounds_kernel<<<blocks, 256, 0, stream_>>>(pos_a_.ptr, n, dp_.cell_size, keys_[0].ptr, st_.ptr);
     compressed_keys_hist_kernel<<<blocks, 256, 0, stream_>>>(pos_a_.ptr, n, dp_.cell_size, st_.ptr, ckeys_.ptr,
                                                              hist_.ptr);
