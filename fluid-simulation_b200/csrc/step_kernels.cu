@@ -40,15 +40,16 @@ __global__ void __launch_bounds__(WPB * 32, KindCfg<KIND>::min_warps / WPB) cell
 
 
 // Resident warps per SM the register allocation of the list kernels must
-// allow (32 -> 64 registers, 36 -> 56, 40 -> 48, 48 -> 42). Both passes wait
-// on neighbour gathers, so resident warps pay as long as nothing spills: the
-// single-scene force pass fits 56 registers (36 warps; at 48 it spills), the
+// allow (36 -> 56 registers, 44 -> 46, 48 -> 42). Both passes wait on
+// neighbour gathers, so resident warps pay while spills stay small: the
+// force pass fits 56 registers (36 warps; at 48 it spills), the single-scene
 // surface pass 40 (50 warps with two-warp blocks, against 40 at the 47 it
-// takes when allowed 48). The batched passes, with the scene lookups, would
-// spill at those caps and keep 64 / 48.
+// takes when allowed 48). The batched passes carry the scene lookups: 56
+// registers cost the force pass 4 bytes of spills and still gain (ensemble
+// step 5.34 -> 5.27 ms); the batched surface pass runs at a 44-warp cap.
 template <int KIND, bool BATCH>
 struct ListCfg {
-    static constexpr int min_warps = BATCH ? (KIND == PASS_FORCE ? 32 : 40) : (KIND == PASS_FORCE ? 36 : 48);
+    static constexpr int min_warps = KIND == PASS_FORCE ? 36 : (BATCH ? 44 : 48);
 };
 
 // Force / surface pass over the neighbour lists written by the density pass.
