@@ -135,6 +135,7 @@ struct BatchSim {
         a.boundary = HashView{btable.ptr, bcstart.ptr, bcend.ptr, btable_size ? btable_size - 1 : 0};
         a.bcell = bcells.view();
         a.bcx = bcells.x.ptr;
+        a.bcx_n = static_cast<u32>(bcells.x.count);
         a.bmask = (bcells.size && mask_words >= 4 && dp.cell_size == dp.h) ? bmask.ptr : nullptr;
         a.mask = mask.ptr;
         a.mask_words = static_cast<u32>(mask_words);
@@ -280,6 +281,7 @@ struct BatchSim {
             if (flags & ERR_LOOKBACK_TIMEOUT) throw Error(WCSPH_ERR_DEVICE_TIMEOUT, "radix sort look-back timed out");
             if (flags & ERR_BARRIER_TIMEOUT)
                 throw Error(WCSPH_ERR_DEVICE_TIMEOUT, "persistent ensemble kernel: grid barrier timed out");
+            if (flags & ERR_BOUNDS) throw Error(WCSPH_ERR_BOUNDS, "device index out of bounds (bounds-checked build)");
             throw Error(WCSPH_ERR_NEIGHBOR_OVERFLOW, "boundary candidate cells exceed capacity");
         }
     }

@@ -96,6 +96,7 @@ const char* wcsph_status_string(int s) {
     case WCSPH_ERR_CONFIG: return "bad tuning configuration";
     case WCSPH_ERR_NOT_SUPPORTED: return "not supported";
     case WCSPH_ERR_STATE: return "invalid state";
+    case WCSPH_ERR_BOUNDS: return "device index out of bounds (bounds-checked build)";
     default: return "unknown status";
     }
 }

@@ -279,6 +279,7 @@ void CUDASPHSimulator::check_device_errors() {
         if (flags & ERR_HASH_FULL) throw Error(WCSPH_ERR_HASH_FULL, "spatial hash table is full (raise table_size_mult)");
         if (flags & ERR_LOOKBACK_TIMEOUT) throw Error(WCSPH_ERR_DEVICE_TIMEOUT, "radix sort look-back wait timed out");
         if (flags & ERR_CAND_OVERFLOW) throw Error(WCSPH_ERR_NEIGHBOR_OVERFLOW, "boundary candidate cells exceed capacity");
+        if (flags & ERR_BOUNDS) throw Error(WCSPH_ERR_BOUNDS, "device index out of bounds (bounds-checked build)");
     }
 }
 
@@ -296,6 +297,7 @@ TravArgs CUDASPHSimulator::trav_args(float delta) {
     a.boundary = HashView{btable_.ptr, bcstart_.ptr, bcend_.ptr, btable_size_ ? btable_size_ - 1 : 0};
     a.bcell = bcells_.view();
     a.bcx = bcells_.x.ptr;
+    a.bcx_n = static_cast<u32>(bcells_.x.count);
     // the density pass writes the masks where it reads the runs (cell size h);
     // they are built in its bit-matrix scratch (4 words per row)
     a.bmask = (bcells_.size && cfg_.mask_words >= 4 && dp_.cell_size == dp_.h) ? bmask_.ptr : nullptr;

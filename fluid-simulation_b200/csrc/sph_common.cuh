@@ -311,6 +311,7 @@ enum : u32 {
     ERR_LOOKBACK_TIMEOUT = 2u,
     ERR_CAND_OVERFLOW = 4u,
     ERR_BARRIER_TIMEOUT = 8u,   // a grid barrier of the persistent ensemble kernel waited too long
+    ERR_BOUNDS = 16u,           // bounds-checked build: an index guard fired
 };
 
 }  // namespace wcsph

@@ -30,6 +30,27 @@
 namespace wcsph {
 namespace {
 
+// Index guards of the bounds-checked build (compiled with WCSPH_CHECKS=1:
+// `make checked`, lib/libwcsph_checked.so). An index at or past its bound
+// raises ERR_BOUNDS in the step's error flags and is replaced by 0, so that
+// the access stays inside its buffer and nothing faults; the host then
+// reports WCSPH_ERR_BOUNDS. The default build compiles the guards away.
+#ifndef WCSPH_CHECKS
+#define WCSPH_CHECKS 0
+#endif
+__device__ __forceinline__ u32 guard_st(DevState* st, u32 idx, u32 bound) {
+#if WCSPH_CHECKS
+    if (idx >= bound) {
+        atomicOr(&st->error_flags, ERR_BOUNDS);
+        return 0u;
+    }
+#else
+    (void)st;
+    (void)bound;
+#endif
+    return idx;
+}
+
 template <class T>
 __device__ __forceinline__ T ro_ld(const T* p) {
 #if WCSPH_COHERENT_LOADS
@@ -37,6 +58,13 @@ __device__ __forceinline__ T ro_ld(const T* p) {
 #else
     return __ldg(p);
 #endif
+}
+
+__device__ __forceinline__ u32 guard(const TravArgs& a, u32 idx, u32 bound) { return guard_st(a.st, idx, bound); }
+// Cells of the staged neighbourhood ranges: (2R + 1)^3, or the 36 of an x-pair union.
+__device__ __forceinline__ u32 range_cells(const TravArgs& a) {
+    const u32 d = 2u * static_cast<u32>(a.range) + 1u;
+    return max(d * d * d, 36u);
 }
 
 // Linear-probed lookup of a packed cell key (find_cell_in_table,
@@ -279,8 +307,8 @@ __device__ __forceinline__ void stage(const WarpView<KIND>& S, const TravArgs& a
             src = S.rstart[q] + (lo - b);
         }
         for (u32 t = sub; lo + t < hi; t += lpc) {
-            const u32 j = src + t;
-            const u32 ml = lo + t - c0;
+            const u32 j = guard(a, src + t, a.n);
+            const u32 ml = guard(a, lo + t - c0, a.mask_words * 32u);
             if constexpr (KindCfg<KIND>::stage_j) S.cand[ml] = j;
             if constexpr (KindCfg<KIND>::stage_q) S.cq[ml] = static_cast<unsigned char>(q);
             if constexpr (KindCfg<KIND>::stage_sa) S.sa[ml] = ro_ld(a.pos + j);
@@ -317,6 +345,7 @@ __device__ __forceinline__ void load_record(const float4* r, float4& x, float4& 
 template <int KIND>
 __device__ __forceinline__ Nbr fetch_j(const TravArgs& a, u32 j) {
     Nbr d;
+    j = guard(a, j, a.n);
     d.j = j;
     load_record((KIND == PASS_FORCE ? a.recf : a.recs) + 2 * static_cast<size_t>(j), d.x, d.b);
     d.c = d.x.w;
@@ -326,6 +355,7 @@ __device__ __forceinline__ Nbr fetch_j(const TravArgs& a, u32 j) {
 template <int KIND>
 __device__ __forceinline__ Nbr fetch(const WarpView<KIND>& S, const TravArgs& a, u32 m) {
     Nbr d;
+    m = guard(a, m, a.mask_words * 32u);
     if constexpr (KindCfg<KIND>::soa) {
         const float* f = reinterpret_cast<const float*>(S.sp + pair_slot(m >> 1)) + (m & 1u);
         d.x = make_float4(f[0], f[2], f[4], 0.f);
@@ -378,6 +408,7 @@ struct HomeData {
 template <int KIND>
 __device__ __forceinline__ HomeData load_home(const TravArgs& a, u32 i) {
     HomeData H;
+    i = guard(a, i, a.n);
     if constexpr (KIND == PASS_FORCE) {
         load_record(a.recf + 2 * static_cast<size_t>(i), H.x, H.v);   // x.w = p / rho^2
         H.prs = ro_ld(a.prs + i);
@@ -574,7 +605,7 @@ __device__ __forceinline__ void boundary_pair_m(float* v, const HomeData& H, flo
 template <int KIND>
 __device__ __forceinline__ void boundary_pair(float* v, const HomeData& H, u32 b, float4 xb, float r2,
                                               const DevParams& P, const TravArgs& a) {
-    boundary_pair_m<KIND>(v, H, ro_ld(a.bmass + b), xb, r2, P);
+    boundary_pair_m<KIND>(v, H, ro_ld(a.bmass + guard(a, b, a.nb)), xb, r2, P);
 }
 
 // Boundary key of cell c (cell size h) of the scene.
@@ -677,11 +708,11 @@ __device__ __forceinline__ u32 fluid_pair_run(const WarpView<KIND>& S, const Dev
 __device__ __forceinline__ float4 home_x(const WarpView<PASS_DENSITY>& S, const TravArgs& a, u32 i0, HomeMap hm,
                                          u32 k) {
     if (hm.c1 != NO_HOME) {
-        const u32 m = hm.cand(k);
+        const u32 m = guard(a, hm.cand(k), a.mask_words * 32u);
         const float* f = reinterpret_cast<const float*>(S.sp + pair_slot(m >> 1)) + (m & 1u);
         return make_float4(f[0], f[2], f[4], 0.f);
     }
-    return ro_ld(a.pos + i0 + k);
+    return ro_ld(a.pos + guard(a, i0 + k, a.n));
 }
 
 // Neighbour pairs of rows [0, nh) read from the block's bit matrix in
@@ -772,9 +803,9 @@ __device__ __forceinline__ u32 fluid_hit_run(const WarpView<KIND>& S, const DevP
             if constexpr (KIND == PASS_DENSITY) {
                 const u32 slot = h - slot_base;
                 if (lists && slot < a.nbr_width) {
-                    const u32 m = p - row0;
-                    const u32 q = S.cq[m];
-                    a.nbr[slot * a.n + i0 + k] = S.rstart[q] + (m - S.rpref[q]);
+                    const u32 m = guard(a, p - row0, a.mask_words * 32u);
+                    const u32 q = guard(a, S.cq[m], range_cells(a));
+                    a.nbr[slot * a.n + guard(a, i0 + k, a.n)] = S.rstart[q] + (m - S.rpref[q]);
                 }
             }
             const Nbr d = fetch<KIND>(S, a, p - row0);
@@ -847,7 +878,7 @@ __device__ __forceinline__ u32 boundary_pair_run(const WarpView<KIND>& S, const 
 #pragma unroll
         for (int f = 0; f < NFB; ++f) v[f] = 0.f;
         for (;;) {
-            const u32 b = S.bcand[m];
+            const u32 b = guard(a, S.bcand[m], a.nb);
             const float4 xb = ro_ld(a.bpos + b);
             const float r2 = dist2(H.x, xb);
             if (r2 <= P.h2) boundary_pair<KIND>(v, H, b, xb, r2, P, a);
@@ -899,13 +930,13 @@ __device__ __forceinline__ u32 boundary_cells_run(const WarpView<KIND>& S, const
             m = q - (k - split) * lb;
         }
         u32 len = k < split ? la : lb;
-        const float4* run = a.bcx + (k < split ? sa : sb);
+        u32 run = k < split ? sa : sb;
         HomeData H = load_home<KIND>(a, i0 + k);
         float v[NFB];
 #pragma unroll
         for (int f = 0; f < NFB; ++f) v[f] = 0.f;
         for (;;) {
-            const float4 xb = ro_ld(run + m);
+            const float4 xb = ro_ld(a.bcx + guard(a, run + m, a.bcx_n));
             const float r2 = dist2(H.x, xb);
             if (r2 <= P.h2) {
                 boundary_pair_m<KIND>(v, H, xb.w, xb, r2, P);
@@ -920,7 +951,7 @@ __device__ __forceinline__ u32 boundary_cells_run(const WarpView<KIND>& S, const
                 m = 0;
                 ++k;
                 len = k < split ? la : lb;
-                run = a.bcx + (k < split ? sa : sb);
+                run = k < split ? sa : sb;
                 H = load_home<KIND>(a, i0 + k);
             }
         }
@@ -1103,14 +1134,14 @@ __device__ __forceinline__ void boundary_row(const DevParams& P, const TravArgs&
 #pragma unroll
             for (u32 w = 0; w < 4; ++w) {
                 for (u32 bits = words[w]; bits; bits &= bits - 1) {
-                    const float4 xb = ro_ld(a.bcx + t + 32u * w + (__ffs(bits) - 1));
+                    const float4 xb = ro_ld(a.bcx + guard(a, t + 32u * w + (__ffs(bits) - 1), a.bcx_n));
                     boundary_pair_m<KIND>(resb, H, xb.w, xb, dist2(H.x, xb), P);
                 }
             }
             return;
         }
         for (; t < e; ++t) {
-            const float4 xb = ro_ld(a.bcx + t);
+            const float4 xb = ro_ld(a.bcx + guard(a, t, a.bcx_n));
             const float r2 = dist2(H.x, xb);
             if (r2 <= P.h2) boundary_pair_m<KIND>(resb, H, xb.w, xb, r2, P);
         }
@@ -1127,7 +1158,7 @@ __device__ __forceinline__ void boundary_row(const DevParams& P, const TravArgs&
                 if (slot == EMPTY_CELL) continue;
                 const u32 e = ro_ld(a.boundary.cend + slot);
                 for (u32 b = ro_ld(a.boundary.cstart + slot); b < e; ++b) {
-                    const float4 xb = ro_ld(a.bpos + b);
+                    const float4 xb = ro_ld(a.bpos + guard(a, b, a.nb));
                     const float r2 = dist2(H.x, xb);
                     if (r2 <= P.h2) boundary_pair<KIND>(resb, H, b, xb, r2, P, a);
                 }
@@ -1648,7 +1679,7 @@ __device__ __forceinline__ void reorder_cell_item(const float4* WCSPH_RESTRICT p
     const bool valid = i < n;
     u64 pk = 0;
     if (valid) {
-        const u32 src = perm ? perm[i] : i;
+        const u32 src = guard_st(st_err, perm ? perm[i] : i, n);
         const float4 p = pos_in[src];
         pos_out[i] = p;
         if (vel_out) vel_out[i] = vel_in[src];
@@ -1659,11 +1690,11 @@ __device__ __forceinline__ void reorder_cell_item(const float4* WCSPH_RESTRICT p
     u64 prev = __shfl_up_sync(FULL, pk, 1);
     u64 next = __shfl_down_sync(FULL, pk, 1);
     if (valid && lane == 0 && i > 0) {
-        const u32 s2 = perm ? perm[i - 1] : i - 1;
+        const u32 s2 = guard_st(st_err, perm ? perm[i - 1] : i - 1, n);
         prev = cell_key_of<BATCH>(pos_in[s2], cs, scene_in, s2);
     }
     if (valid && lane == 31 && i + 1 < n) {
-        const u32 s2 = perm ? perm[i + 1] : i + 1;
+        const u32 s2 = guard_st(st_err, perm ? perm[i + 1] : i + 1, n);
         next = cell_key_of<BATCH>(pos_in[s2], cs, scene_in, s2);
     }
     if (!valid) return;

@@ -76,6 +76,7 @@ struct TravArgs {
     // nullptr: not built, the passes look the 27 boundary cells up)
     HashView bcell;
     const float4* bcx;
+    u32 bcx_n;                // entries of bcx
     // per sorted particle: bit m set when candidate m (< 128) of its cell's
     // run is within h; written by the density pass, read by the force pass
     // (nullptr: the force pass tests the whole run)

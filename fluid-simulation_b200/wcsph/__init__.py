@@ -27,7 +27,10 @@ from pathlib import Path
 import numpy as np
 
 _PKG_ROOT = Path(__file__).resolve().parent.parent
-LIB_PATH = _PKG_ROOT / "lib" / "libwcsph.so"
+# WCSPH_LIBRARY selects another build of the same ABI for a process, e.g. the
+# bounds-checked lib/libwcsph_checked.so (`make -C fluid-simulation_b200 checked`).
+CHECKED_LIB_PATH = _PKG_ROOT / "lib" / "libwcsph_checked.so"
+LIB_PATH = Path(os.environ["WCSPH_LIBRARY"]) if os.environ.get("WCSPH_LIBRARY") else _PKG_ROOT / "lib" / "libwcsph.so"
 HEADER_PATH = _PKG_ROOT.parent / "include" / "wcsph.h"
 
 # ---- status codes (enum wcsph_status) ---------------------------------------
@@ -48,6 +51,7 @@ ERR_NO_DEVICE = 13
 ERR_CONFIG = 14
 ERR_NOT_SUPPORTED = 15
 ERR_STATE = 16
+ERR_BOUNDS = 17   # bounds-checked build only: a device index guard fired
 
 FORCE_NONE, FORCE_CONSTANT, FORCE_FOUNTAIN, FORCE_VORTEX = 0, 1, 2, 3
 SEARCH_MCMC, SEARCH_RANDOM, SEARCH_FULL = 0, 1, 2

@@ -63,7 +63,9 @@ enum wcsph_status {
     WCSPH_ERR_NO_DEVICE = 13,          /* no CUDA device / extension unusable   */
     WCSPH_ERR_CONFIG = 14,             /* bad tuning config / frozen JSON       */
     WCSPH_ERR_NOT_SUPPORTED = 15,
-    WCSPH_ERR_STATE = 16               /* call not valid in the current state   */
+    WCSPH_ERR_STATE = 16,              /* call not valid in the current state   */
+    WCSPH_ERR_BOUNDS = 17              /* bounds-checked build (libwcsph_checked.so):
+                                          a device index guard fired            */
 };
 
 /* ---- external force fields --------------------------------------------

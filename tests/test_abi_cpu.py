@@ -15,6 +15,21 @@ def test_library_exports_every_header_symbol():
     assert lib.wcsph_abi_version() == 1
 
 
+def test_checked_library_exports_every_header_symbol():
+    # the bounds-checked build (`make checked`) has the same ABI
+    path = wcsph.CHECKED_LIB_PATH
+    if not path.exists():
+        import pytest
+
+        pytest.skip("lib/libwcsph_checked.so is not built (make -C fluid-simulation_b200 checked)")
+    lib = C.CDLL(str(path))
+    missing = [s for s in wcsph.header_symbols() if not hasattr(lib, s)]
+    assert missing == []
+    assert lib.wcsph_abi_version() == 1
+    lib.wcsph_status_string.restype = C.c_char_p
+    assert b"bounds" in lib.wcsph_status_string(wcsph.ERR_BOUNDS)
+
+
 def test_default_params_are_the_reference_constants():
     p = wcsph.default_params()
     # common.cuh:18-23, compute_rho_p.cu:10-12, compute_non_pressure_accel.cu:14-16,
