@@ -43,6 +43,9 @@ def _scenes(out):
         for k in range(len(pres)):
             res[f"ens{int(persistent)}_{k}_pos"], res[f"ens{int(persistent)}_{k}_vel"] = b.get_state(k)
         b.close()
+    # the library this process mapped (the parent checks it is the one it asked for)
+    maps = Path("/proc/self/maps").read_text()
+    res["mapped"] = np.array(sorted({ln.split()[-1] for ln in maps.splitlines() if "libwcsph" in ln}))
     np.savez(out, **res)
 
 
@@ -50,7 +53,9 @@ def _run(lib, out):
     env = dict(os.environ, WCSPH_LIBRARY=str(lib))
     r = subprocess.run([sys.executable, __file__, str(out)], env=env, capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
-    return np.load(out)
+    d = np.load(out)
+    assert [Path(m).name for m in d["mapped"]] == [Path(lib).name], d["mapped"]
+    return d
 
 
 def test_checked_build_is_silent_and_bit_identical(tmp_path):
@@ -62,6 +67,8 @@ def test_checked_build_is_silent_and_bit_identical(tmp_path):
     want = _run(lib_dir / "libwcsph.so", tmp_path / "default.npz")
     assert sorted(got.files) == sorted(want.files)
     for k in want.files:
+        if k == "mapped":
+            continue
         assert np.array_equal(got[k].view(np.uint32), want[k].view(np.uint32)), k
 
 
