@@ -14,8 +14,12 @@
 //
 // Build (stream-ordered, once per boundary):
 //   1. count the occupied boundary cells (slots of the boundary hash);
-//   2. insert the 27 neighbours of each into the near-cell hash (sized for
-//      27 per occupied cell at half load, so it cannot fill up);
+//   2. insert the 27 neighbours of each into a key-only hash sized for 27
+//      per occupied cell at half load (so it cannot fill up), count the
+//      distinct near cells, and move them into the near-cell hash proper,
+//      sized for them at a quarter load (walls have 3-5 near cells per
+//      occupied cell, so this table is several times smaller; at half load
+//      the longer probe chains cost 0.5 % of the ensemble step);
 //   3. per near cell, the candidate count (27 lookups in the boundary hash);
 //   4. exclusive scan of the counts (CUB) -> run starts; total read back;
 //   5. per near cell, copy its candidates into its run.
@@ -61,6 +65,14 @@ __global__ void near_insert_kernel(const u64* __restrict__ btable, u32 bsize, u6
         for (int q = 0; q < 27; ++q)
             if (hash_insert<BATCH>(near, nmask, neighbour_key<BATCH>(pk, q)) == EMPTY_CELL)
                 atomicOr(&st->error_flags, ERR_HASH_FULL);
+    }
+}
+
+template <bool BATCH>
+__global__ void rehash_kernel(const u64* __restrict__ from, u32 fsize, u64* to, u32 tmask, DevState* st) {
+    for (u32 t = blockIdx.x * blockDim.x + threadIdx.x; t < fsize; t += gridDim.x * blockDim.x) {
+        const u64 pk = from[t];
+        if (pk != EMPTY_HASH && hash_insert<BATCH>(to, tmask, pk) == EMPTY_CELL) atomicOr(&st->error_flags, ERR_HASH_FULL);
     }
 }
 
@@ -118,15 +130,31 @@ void build_boundary_cells(BoundaryCells& bc, const HashView& bh, u32 bsize, u32 
     WCSPH_CUDA(cudaMemcpyAsync(&cells, counter.ptr, sizeof(u32), cudaMemcpyDeviceToHost, s));
     WCSPH_CUDA(cudaStreamSynchronize(s));
     if (cells == 0 || 54ull * cells > (1ull << 31)) return;
-    const u32 nsize = static_cast<u32>(std::bit_ceil(std::max<u64>(64, 54ull * cells)));
-    bc.table.alloc(nsize);
+    u32 nsize = 0;
+    {
+        const u32 wsize = static_cast<u32>(std::bit_ceil(std::max<u64>(64, 54ull * cells)));
+        DevBuf<u64> wide(wsize);
+        WCSPH_CUDA(cudaMemsetAsync(wide.ptr, 0xff, wide.bytes(), s));
+        if (batch) near_insert_kernel<true><<<grid_for(bsize), 256, 0, s>>>(bh.table, bsize, wide.ptr, wsize - 1, st);
+        else near_insert_kernel<false><<<grid_for(bsize), 256, 0, s>>>(bh.table, bsize, wide.ptr, wsize - 1, st);
+        WCSPH_CUDA(cudaGetLastError());
+        WCSPH_CUDA(cudaMemsetAsync(counter.ptr, 0, sizeof(u32), s));
+        count_cells_kernel<<<grid_for(wsize), 256, 0, s>>>(wide.ptr, wsize, counter.ptr);
+        WCSPH_CUDA(cudaGetLastError());
+        u32 near = 0;
+        WCSPH_CUDA(cudaMemcpyAsync(&near, counter.ptr, sizeof(u32), cudaMemcpyDeviceToHost, s));
+        WCSPH_CUDA(cudaStreamSynchronize(s));
+        nsize = static_cast<u32>(std::bit_ceil(std::max<u64>(64, 4ull * near)));
+        bc.table.alloc(nsize);
+        WCSPH_CUDA(cudaMemsetAsync(bc.table.ptr, 0xff, bc.table.bytes(), s));
+        if (batch) rehash_kernel<true><<<grid_for(wsize), 256, 0, s>>>(wide.ptr, wsize, bc.table.ptr, nsize - 1, st);
+        else rehash_kernel<false><<<grid_for(wsize), 256, 0, s>>>(wide.ptr, wsize, bc.table.ptr, nsize - 1, st);
+        WCSPH_CUDA(cudaGetLastError());
+        WCSPH_CUDA(cudaStreamSynchronize(s));   // before the wide table is freed
+    }
     bc.start.alloc(nsize);
     bc.end.alloc(nsize);
     bc.size = nsize;
-    WCSPH_CUDA(cudaMemsetAsync(bc.table.ptr, 0xff, bc.table.bytes(), s));
-    if (batch) near_insert_kernel<true><<<grid_for(bsize), 256, 0, s>>>(bh.table, bsize, bc.table.ptr, nsize - 1, st);
-    else near_insert_kernel<false><<<grid_for(bsize), 256, 0, s>>>(bh.table, bsize, bc.table.ptr, nsize - 1, st);
-    WCSPH_CUDA(cudaGetLastError());
     DevBuf<u32> count(nsize);
     if (batch) near_count_kernel<true><<<grid_for(nsize), 256, 0, s>>>(bh, bc.table.ptr, nsize, count.ptr);
     else near_count_kernel<false><<<grid_for(nsize), 256, 0, s>>>(bh, bc.table.ptr, nsize, count.ptr);
